@@ -1,0 +1,161 @@
+#!/usr/bin/env python3
+"""Recipe that compiles the HARM3D reference's own CPU step into oracle/_ref/.
+
+This is test infrastructure: it produces the reference executables that pin
+the C oracle (oracle/harm_oracle.c) and the golden fixtures under
+tests/golden/.  Nothing in the product (coolharm3d_b200/) links or runs them.
+
+What it does, per configuration:
+  1. stages the reference's src/ files into oracle/_ref/<cfg>/src/
+     (a git-ignored build folder; reference sources are never committed),
+  2. applies the documented compile-time switch edits to the staged
+     options.h (each edit is listed in CONFIGS below and in DESIGN.md),
+     and the documented parameter edits to the staged init.<setup>.c,
+  3. regenerates defs.h from globals.h exactly as the reference makefile
+     does (src/makefile, the `egrep "^extern|^#if..." globals.h | sed` rule),
+  4. compiles every source of src/makefile:364-373 except corona*.c, plus
+     oracle/ref_probe.c (our harness hook), with
+       gcc -O3 -fcommon -ffp-contract=off
+     step_ch.c is compiled with -Dstep_ch=ref_step_ch so that the reference's
+     own main() loop calls the probe's step_ch(), which wraps the real one,
+     dumps state and optionally loads an initial state (see ref_probe.c).
+
+Usage:  python oracle/build_ref.py [cfg ...]   (default: all configs)
+The reference tree is read from $HARM_REF_SRC or /root/reference/src.
+"""
+import os
+import re
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+REF_SRC = os.environ.get("HARM_REF_SRC", "/root/reference/src")
+
+# src/makefile:364-373, minus corona.c corona2.c (cooling choices 4/5 only)
+# and minus the init file (one init.*.c is linked per configuration).
+BASE_SRCS = [
+    "bounds.c", "coord.c", "diag.c", "dump.c", "fixup.c", "flux_ct.c", "image.c",
+    "lu.c", "main.c", "metric.c", "phys.c", "ranc.c", "restart.c", "recon.c",
+    "step_ch.c", "u2p_util.c", "utoprim_1d_ee.c", "utoprim_1d_ee2.c",
+    "utoprim_1dfix1.c", "utoprim_1dvsq2fix1.c", "utoprim_1d.c",
+    "utoprim_2d_fast.c", "harm_mpi.c", "dump_hdf.c", "dump_history.c",
+    "dump_stat.c", "dump_stat2.c", "dump_radflux.c", "dump_surface.c",
+    "dump_timers.c", "decomp.c", "dump_photosphere.c", "interp_data.c",
+]
+
+# Output-only switches turned off in every configuration (no HDF5 in the image).
+IO_OFF = {
+    "MAKE_HISTORY": "0", "MAKE_HDF5": "0", "MAKE_STAT": "0", "MAKE_RADFLUX": "0",
+    "MAKE_PHOTOSPHERE": "0", "MAKE_ASCII": "0", "MAKE_IMAGE": "0",
+}
+
+MINK = {
+    "METRIC_TYPE_CHOICE": "(METRIC_MINK_CARTESIAN)",
+    "COORD_TYPE_CHOICE": "(COORD_IDENTITY)",
+    "USE_COOLING_FUNCTION": "(0)",
+    "RESCALE_R": "(0)",
+}
+
+# name -> (init file, options.h edits, init-file literal edits)
+CONFIGS = {
+    # Balsara test 1, 1D shock tube: MC + HLLE + para flux-CT, outflow.
+    "balsara1": ("init.balsara1.c",
+                 dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_OUTFLOW)",
+                      RECON_TYPE_CHOICE="(RECON_MC)", FLUX_TYPE_CHOICE="(FLUX_HLLE)"),
+                 [("cour = 0.8 ;", "cour = 0.5 ;")]),
+    # Same physics with the shipped Courant number, LF flux and minmod slopes,
+    # plain Toth flux-CT: exercises the alternative switches of the step.
+    "balsara1_lf": ("init.balsara1.c",
+                    dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_OUTFLOW)",
+                         RECON_TYPE_CHOICE="(RECON_MINMOD)", FLUX_TYPE_CHOICE="(FLUX_LF)",
+                         USE_FLUX_CT_PARA="(0)"),
+                    []),
+    # Periodic linear wave (the reference's 2D slow mode): PPM_MC + HLLE.
+    "linwave": ("init.linearwave.c",
+                dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)",
+                     RECON_TYPE_CHOICE="(RECON_PPM_MC)", FLUX_TYPE_CHOICE="(FLUX_HLLE)"),
+                []),
+    # Same setup with van Leer PPM limiter and LF flux.
+    "linwave_vl": ("init.linearwave.c",
+                   dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)",
+                        RECON_TYPE_CHOICE="(RECON_PPM_VL)", FLUX_TYPE_CHOICE="(FLUX_LF)"),
+                   []),
+}
+
+
+def set_define(text, name, value):
+    pat = re.compile(r"^(#define\s+%s\s+)(.*)$" % re.escape(name), re.M)
+    if not pat.search(text):
+        raise SystemExit("build_ref: no '#define %s' in options.h" % name)
+    return pat.sub(lambda m: m.group(1) + value, text, count=1)
+
+
+def stage(cfg):
+    init_file, opts, init_edits = CONFIGS[cfg]
+    bdir = os.path.join(OUT, cfg)
+    sdir = os.path.join(bdir, "src")
+    if os.path.isdir(sdir):
+        shutil.rmtree(sdir)
+    os.makedirs(sdir)
+    for f in os.listdir(REF_SRC):
+        if f.endswith((".c", ".h")):
+            shutil.copy(os.path.join(REF_SRC, f), sdir)
+    opt_path = os.path.join(sdir, "options.h")
+    text = open(opt_path).read()
+    for k, v in dict(IO_OFF, **opts).items():
+        text = set_define(text, k, v)
+    open(opt_path, "w").write(text)
+    ipath = os.path.join(sdir, init_file)
+    itext = open(ipath).read()
+    for old, new in init_edits:
+        if old not in itext:
+            raise SystemExit("build_ref: edit target %r not in %s" % (old, init_file))
+        itext = itext.replace(old, new, 1)
+    open(ipath, "w").write(itext)
+    # defs.h: same transform as the reference makefile's defs.h rule.
+    defs = []
+    for line in open(os.path.join(sdir, "globals.h")):
+        if re.match(r"^(extern|#if|#elif|#else|#endif)", line):
+            defs.append(re.sub(r"^extern", "", line, count=1))
+    open(os.path.join(sdir, "defs.h"), "w").write("".join(defs))
+    return bdir, sdir, init_file
+
+
+def build(cfg, jobs=8):
+    bdir, sdir, init_file = stage(cfg)
+    odir = os.path.join(bdir, "obj")
+    os.makedirs(odir, exist_ok=True)
+    cflags = ["-O3", "-fcommon", "-ffp-contract=off", "-w", "-I", sdir]
+    srcs = [os.path.join(sdir, s) for s in BASE_SRCS + [init_file]]
+    srcs.append(os.path.join(HERE, "ref_probe.c"))
+    procs, objs = [], []
+    for s in srcs:
+        o = os.path.join(odir, os.path.basename(s)[:-2] + ".o")
+        extra = ["-Dstep_ch=ref_step_ch"] if os.path.basename(s) == "step_ch.c" else []
+        objs.append(o)
+        procs.append(subprocess.Popen(["gcc"] + cflags + extra + ["-c", s, "-o", o]))
+        if len(procs) >= jobs:
+            if procs.pop(0).wait() != 0:
+                raise SystemExit("build_ref: compile failed for " + cfg)
+    for p in procs:
+        if p.wait() != 0:
+            raise SystemExit("build_ref: compile failed for " + cfg)
+    exe = os.path.join(bdir, "harm3d")
+    subprocess.check_call(["gcc", "-o", exe] + objs + ["-lm"])
+    return exe
+
+
+def main(argv):
+    cfgs = argv or sorted(CONFIGS)
+    if not os.path.isdir(REF_SRC):
+        print("build_ref: reference sources not found at %s; skipping" % REF_SRC)
+        return 0
+    for c in cfgs:
+        print("built", build(c))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))
