@@ -1,0 +1,350 @@
+#!/usr/bin/env python3
+"""Benchmark of the HARM3D step engine: zone-updates/s on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+A step is one full RK2 step_ch() of the grid (predictor + corrector with
+boundaries, fixups and the CFL reduction).  Rank 0 prints one JSON line.
+
+Workloads (synthetic data of the configuration's shape; no dataset involved):
+  linwave256  3D periodic Minkowski linear wave, 256^3 zones, Gamma=4/3,
+              rho=1, p=1, B=(1,1.5,0), plane-wave perturbation of amplitude
+              1e-6 along the grid diagonal; PPM_MC + HLLE + para flux-CT, FP64.
+
+Multi-GPU (torchrun): the path does not shard across GPUs in this engine
+(one grid per GPU); every rank advances its own replica, time = max over
+ranks, value = total zone-updates of all ranks / that time ("weak").
+
+The reference arm (--impl reference) times the reference's own CPU build
+(oracle/_ref/<config>/harm3d, made from the reference sources by
+oracle/build_ref.py) on the host cores: one process per core, each the
+64^3 block one rank of a 4x4x4 decomposition of the 256^3 grid would own,
+run without MPI (no halo exchange, so an upper bound on the MPI build).
+"""
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+PEAKS_FILE = os.path.join(HERE, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="linwave256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+WORKLOADS = {
+    "linwave256": dict(n=(256, 256, 256), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
+                       ref_block=(64, 64, 64),
+                       label="3D periodic Minkowski linear wave 256^3, PPM_MC+HLLE+para flux-CT, FP64"),
+    "linwave128": dict(n=(128, 128, 128), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
+                       ref_block=(32, 32, 32),
+                       label="3D periodic Minkowski linear wave 128^3, PPM_MC+HLLE+para flux-CT, FP64"),
+}
+
+
+def linwave_state(n, gam):
+    """rho=1, p=1, B=(1,1.5,0) plus a diagonal plane wave of amplitude 1e-6."""
+    import coolharm3d_b200 as hg
+    shape = hg.ref_shape(n)
+    dx = [1.0 / x for x in n]
+    x = -3 * dx[0] + (np.arange(shape[0]) + 0.5) * dx[0]
+    y = -3 * dx[1] + (np.arange(shape[1]) + 0.5) * dx[1]
+    z = -3 * dx[2] + (np.arange(shape[2]) + 0.5) * dx[2]
+    ph = np.cos(2 * np.pi * (x[:, None, None] + y[None, :, None] + z[None, None, :]))
+    amp = 1e-6
+    p = np.empty(shape + (8,))
+    p[..., 0] = 1 + amp * ph
+    p[..., 1] = 1.0 / (gam - 1.0) + amp * 3.0 * ph
+    p[..., 2] = amp * 0.5 * ph
+    p[..., 3] = amp * 0.5 * ph
+    p[..., 4] = amp * -0.2 * ph
+    p[..., 5] = 1.0 + amp * 0.3 * ph
+    p[..., 6] = 1.5 - amp * 0.2 * ph
+    p[..., 7] = amp * 0.7 * ph
+    return p
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peak_hbm():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def algorithmic_bytes(kind, n):
+    """Algorithmic HBM bytes of one launch of a kernel class (FP64 state).
+
+    flux (one direction): every zone of the stencil box read once (8 prims)
+    plus the 8 flux components written once per face.  update: p, p_h read,
+    five non-induction flux components of the three face families, three
+    EMFs and two floors read once per zone; p_f (8), p_gamma and pflag
+    written once per zone."""
+    N0, N1, N2 = n
+    T = [x + 6 for x in n]
+    if kind == "flux":
+        faces = (N0 + 1) * T[1] * T[2]
+        return 64.0 * T[0] * T[1] * T[2] + 64.0 * faces
+    if kind == "update":
+        return (64 + 64 + 3 * 40 + 24 + 16 + 64 + 8 + 4) * float(N0 * N1 * N2)
+    if kind == "emf":
+        return (6 * 8 + 3 * 8) * float((N0 + 1) * (N1 + 1) * (N2 + 1))
+    return None
+
+
+def run_ours(args, wl, rank, world, device):
+    import coolharm3d_b200 as hg
+    n = wl["n"]
+    dx = [1e-5] + [1.0 / x for x in n]
+    startx = [0.0] + [-3 * d for d in dx[1:]]
+    desc = hg.make_desc(n, wl["gam"], wl["cour"], dx, startx, [1e9, 1, 1, 1], recon=wl["recon"], flux=wl["flux"],
+                        bc=wl["bc"], device=device)
+    geom, cell6 = hg.minkowski_tables(desc)
+    p0 = linwave_state(n, wl["gam"])
+    e = hg.Engine(desc)
+    e.set_geometry(geom)
+    e.set_cell_data(cell6)
+    e.upload(p0)
+    zones = n[0] * n[1] * n[2]
+    barrier, sync = lambda: None, lambda: None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            sync = torch.cuda.synchronize
+        if world > 1:
+            import torch.distributed as dist
+            barrier = dist.barrier
+    except ImportError:
+        pass
+    e.step(args.warmup)
+    # timed region: K steps on the device, state resident (inputs > L2: 1.1 GB per state array)
+    e.profile(True)
+    clk = ClockSampler(device)
+    clk.start()
+    barrier()
+    sync()
+    e.step(args.steps)
+    sync()
+    barrier()
+    clocks = clk.stop()
+    ms = e.last_step_ms()
+    kt = e.kernel_times()
+    e.profile(False)
+    # end to end through the C ABI with host buffers: upload from host, K x
+    # (hg_step + t/dt + nfailtot readback, what step_ch()'s caller needs every
+    # step), download to host -- all inside the timed region
+    host_p = np.ascontiguousarray(p0)
+    t0 = time.perf_counter()
+    e.upload(host_p)
+    for _ in range(args.steps):
+        e.step(1)
+        e.fail_counts()
+    back = e.download()
+    e2e_s = time.perf_counter() - t0
+    del back
+    ms_all = [ms]
+    e2e_all = [e2e_s]
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        tt = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_all, e2e_all = [float(tt[0])], [float(tt[1])]
+    ms_max, e2e_max = ms_all[0], e2e_all[0]
+    value = world * zones * args.steps / (ms_max * 1e-3)
+    e2e_val = world * zones * args.steps / e2e_max
+    state_bytes = 8 * 8 * np.prod(hg.ref_shape(n))
+    out = dict(metric="zone-updates/s", value=value, unit="zone-updates/s", n_gpus=world, steps=args.steps,
+               warmup=args.warmup, ms_per_step=ms_max / args.steps, higher_is_better=True, scaling="weak",
+               vs_baseline=None, dtype="f64", data="synthetic",
+               config={"workload": args.workload, "description": wl["label"], "grid": list(n),
+                       "zones": zones, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (state arrays 1.1 GB each)",
+                       "e2e": "upload from host once + K x (hg_step(1) + nfailtot readback) + download once"})
+    # roofline of the dominant kernel class (live CUDA events on the engine stream)
+    dom = max(("flux", "update", "emf"), key=lambda c: kt[c][0])
+    avg_ms = kt[dom][0] / max(kt[dom][1], 1)
+    alg = algorithmic_bytes(dom, n)
+    peak, src = peak_hbm()
+    ach = alg / (avg_ms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(HERE, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(args.workload, {}).get(dom)
+        except (OSError, ValueError):
+            traffic = None
+    out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "peak_source": src,
+                       "unit": "GB/s", "frac": ach / peak, "traffic": traffic,
+                       "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": alg,
+                       "kernel_share": {c: kt[c][0] / max(sum(v[0] for v in kt.values()), 1e-30) for c in kt}}
+    out["e2e"] = {"value": e2e_val, "unit": "zone-updates/s",
+                  "h2d_bytes_per_step": float(state_bytes) / args.steps,
+                  "d2h_bytes_per_step": float(state_bytes) / args.steps + 16 + 120}
+    total_launches = sum(v[1] for v in kt.values()) + 2 * args.steps  # k_begin launches are in "misc"
+    out["gpu_launches"] = int(sum(v[1] for v in kt.values()))
+    if clocks:
+        out["clocks"] = clocks
+    return out
+
+
+def reference_exe(cfg):
+    return os.path.join(HERE, "oracle", "_ref", cfg, "harm3d")
+
+
+def run_reference_sample(cfg, block, steps, procs):
+    """Time the reference build: `procs` concurrent processes, each `steps`
+    steps of a `block` grid.  Returns (zone-updates/s summed, seconds)."""
+    exe = reference_exe(cfg)
+    if not os.path.exists(exe):
+        return None, "reference build %s absent (run oracle/build_ref.py where the reference sources are)" % exe
+    env = dict(os.environ, HARM_PROBE_MAXSTEPS=str(steps), HARM_PROBE_TIME="1")
+    tds, ps = [], []
+    for _ in range(procs):
+        td = tempfile.mkdtemp()
+        tds.append(td)
+        ps.append(subprocess.Popen([exe, "1", "1", "1"] + [str(x) for x in block], cwd=td, env=env,
+                                   stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+    rates = []
+    for p in ps:
+        outp, _ = p.communicate(timeout=900)
+        m = re.search(r"probe_time steps=(\d+) seconds=([0-9.eE+-]+) cells=(\d+)", outp)
+        if not m:
+            return None, "reference run produced no timing line"
+        st, sec, cells = int(m.group(1)), float(m.group(2)), int(m.group(3))
+        rates.append(st * cells / sec)
+    return float(sum(rates)), None
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = WORKLOADS[args.workload]
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        procs = max(1, min(ncores, 64))
+        rate, err = run_reference_sample(wl["ref_cfg"], wl["ref_block"], 1, procs)
+        if rate is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
+            return 0
+        # the timed steps of the arm: K bounded samples
+        ks = []
+        for _ in range(max(1, min(args.steps, 2))):
+            r, _ = run_reference_sample(wl["ref_cfg"], wl["ref_block"], 1, procs)
+            ks.append(r)
+        value = float(np.median(ks))
+        zones = np.prod(wl["n"])
+        sample = "%d processes x 1 step of the %s block each (one rank's block of %s), reference CPU build, no MPI" % (
+            procs, "x".join(map(str, wl["ref_block"])), "x".join(map(str, wl["n"])))
+        out = dict(impl="reference", metric="zone-updates/s", value=value, unit="zone-updates/s", n_gpus=world,
+                   steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * zones / value, higher_is_better=True,
+                   scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                   config={"workload": args.workload, "description": wl["label"], "grid": list(wl["n"])},
+                   cpu_baseline={"value": value, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
+                                 "sample": sample},
+                   e2e={"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(out))
+        return 0
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    out = run_ours(args, wl, rank, world, local)
+    if rank == 0 and not args.no_cpu_baseline:
+        procs = max(1, min(ncores, 64))
+        rate, err = run_reference_sample(wl["ref_cfg"], wl["ref_block"], 1, procs)
+        if rate is not None:
+            out["cpu_baseline"] = {"value": rate, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
+                                   "sample": "%d processes x 1 step of a %s block (reference CPU build, no MPI)" % (
+                                       procs, "x".join(map(str, wl["ref_block"])))}
+        else:
+            out["cpu_baseline"] = {"value": None, "unit": "zone-updates/s", "cores": 0, "kind": "reference",
+                                   "sample": err}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,220 @@
+"""coolharm3d_b200 -- B200 (sm_100a) engine for HARM3D's step_ch()/advance() path.
+
+The engine is the in-tree shared library libharmgpu.so (C ABI in
+include/harmgpu.h).  This module is its Python binding, used by the tests and
+bench.py the way the reference's C driver (src/main.c, src/step_ch.c) uses the
+library: describe the grid, hand over geometry and primitives, step, read back.
+
+There is no CPU fallback: if libharmgpu.so is missing or no CUDA device is
+present, Engine() raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libharmgpu.so")
+NG, NP, NFAIL, NGEOM = 3, 8, 15, 42
+
+# options.h switch values accepted by the engine
+RECON_MINMOD, RECON_VANL, RECON_MC, RECON_PPM_MM, RECON_PPM_VL, RECON_PPM_MC = range(6)
+FLUX_LF, FLUX_HLLE = 0, 1
+BC_CARTESIAN_OUTFLOW, BC_CARTESIAN_PERIODIC, BC_SPHERICAL_OUTFLOW3 = 0, 1, 10
+PREC_FP64, PREC_MIXED = 0, 1
+
+# nfail[] slots (macros.h:243-258)
+NFAIL_NAMES = ["FLOOR", "TMAX", "GAMMA_MAX", "GAMMA_CALC", "USE_FULL_INV", "USE_EE", "UTOPRIM",
+               "UTOPRIM_EE", "USE_INTERP_PRIM", "USE_INTERP_V", "INTERP_PRIM", "INTERP_V",
+               "CUTOUT_PRESSURE", "CUTOUT_GAMMA", "CUTOUT_BC"]
+
+
+class GridDesc(ctypes.Structure):
+    """hg_grid_desc of include/harmgpu.h."""
+    _fields_ = [("n1", ctypes.c_int32), ("n2", ctypes.c_int32), ("n3", ctypes.c_int32),
+                ("recon_type", ctypes.c_int32), ("flux_type", ctypes.c_int32),
+                ("use_flux_ct_para", ctypes.c_int32), ("bc_type", ctypes.c_int32),
+                ("metric_dim", ctypes.c_int32), ("use_entropy_eq", ctypes.c_int32),
+                ("cooling", ctypes.c_int32), ("rescale_r", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("gam", ctypes.c_double), ("cour", ctypes.c_double), ("dx", ctypes.c_double * 4),
+                ("startx", ctypes.c_double * 4), ("grid_length", ctypes.c_double * 4),
+                ("t", ctypes.c_double), ("device", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", "hg_download_prims",
+           "hg_upload_prims_tree", "hg_download_prims_tree", "hg_set_time", "hg_step", "hg_get_fail_counts",
+           "hg_download_pflag", "hg_download_gamma", "hg_download_nfail", "hg_get_diag", "hg_last_step_ms",
+           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times"]
+KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libharmgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("libharmgpu.so not found at %s: run coolharm3d_b200/build.py" % path)
+    lib = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    I = ctypes.c_int
+    lib.hg_init.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(P)]
+    lib.hg_set_geometry.argtypes = [P, P, ctypes.c_int64, P, ctypes.c_int64]
+    lib.hg_set_cell_data.argtypes = [P, P, P]
+    for fn in ("hg_upload_prims", "hg_download_prims", "hg_upload_prims_tree", "hg_download_prims_tree",
+               "hg_get_fail_counts", "hg_download_pflag", "hg_download_gamma", "hg_download_nfail",
+               "hg_last_step_ms"):
+        getattr(lib, fn).argtypes = [P, P]
+    lib.hg_set_time.argtypes = [P, ctypes.c_double, ctypes.c_double]
+    lib.hg_step.argtypes = [P, ctypes.c_int32, P, P]
+    lib.hg_get_diag.argtypes = [P, P, P]
+    lib.hg_destroy.argtypes = [P]
+    lib.hg_destroy.restype = None
+    lib.hg_strerror.argtypes = [I]
+    lib.hg_strerror.restype = ctypes.c_char_p
+    lib.hg_build_geometry_minkowski.argtypes = [ctypes.POINTER(GridDesc), P, P]
+    lib.hg_profile.argtypes = [P, ctypes.c_int32]
+    lib.hg_kernel_times.argtypes = [P, P, P]
+    for fn in EXPORTS:
+        if fn not in ("hg_destroy", "hg_strerror"):
+            getattr(lib, fn).restype = I
+    _lib = lib
+    return lib
+
+
+class HarmGPUError(RuntimeError):
+    pass
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = load_library().hg_strerror(rc).decode()
+        raise HarmGPUError("%s failed: %s (%d)" % (what, msg, rc))
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def make_desc(n, gam, cour, dx, startx, grid_length, t=0.0, recon=RECON_PPM_MC, flux=FLUX_HLLE, ct_para=1,
+              bc=BC_CARTESIAN_PERIODIC, metric_dim=0, use_ee=1, cooling=0, rescale_r=0, precision=PREC_FP64,
+              device=0):
+    d = GridDesc()
+    d.n1, d.n2, d.n3 = (int(x) for x in n)
+    d.recon_type, d.flux_type, d.use_flux_ct_para = recon, flux, ct_para
+    d.bc_type, d.metric_dim, d.use_entropy_eq = bc, metric_dim, use_ee
+    d.cooling, d.rescale_r, d.precision = cooling, rescale_r, precision
+    d.gam, d.cour, d.t, d.device = gam, cour, t, device
+    for a in range(4):
+        d.dx[a], d.startx[a], d.grid_length[a] = dx[a], startx[a], grid_length[a]
+    return d
+
+
+def ref_shape(n):
+    return tuple(int(x) + 2 * NG for x in n)
+
+
+def minkowski_tables(desc):
+    """Geometry and per-cell floor tables of Minkowski space (host builder)."""
+    lib = load_library()
+    shp = ref_shape((desc.n1, desc.n2, desc.n3))
+    geom = np.zeros(NGEOM)
+    cell6 = np.zeros(shp + (6,))
+    _check(lib.hg_build_geometry_minkowski(ctypes.byref(desc), _ptr(geom), _ptr(cell6)),
+           "hg_build_geometry_minkowski")
+    return geom, cell6
+
+
+class Engine:
+    """One device-resident grid (an hg_handle)."""
+
+    def __init__(self, desc):
+        self.lib = load_library()
+        self.desc = desc
+        self.n = (desc.n1, desc.n2, desc.n3)
+        self.shape = ref_shape(self.n)
+        h = ctypes.c_void_p()
+        _check(self.lib.hg_init(ctypes.byref(desc), ctypes.byref(h)), "hg_init")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hg_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_geometry(self, geom, conn=None):
+        geom = np.ascontiguousarray(geom, np.float64)
+        ng = geom.size // NGEOM
+        conn = None if conn is None else np.ascontiguousarray(conn, np.float64)
+        nc = 0 if conn is None else conn.size // 64
+        _check(self.lib.hg_set_geometry(self.h, _ptr(geom), ng, _ptr(conn), nc), "hg_set_geometry")
+
+    def set_cell_data(self, cell6, rface=None):
+        cell6 = np.ascontiguousarray(cell6, np.float64)
+        rface = None if rface is None else np.ascontiguousarray(rface, np.float64)
+        self._keep = (cell6, rface)
+        _check(self.lib.hg_set_cell_data(self.h, _ptr(cell6), _ptr(rface)), "hg_set_cell_data")
+
+    def upload(self, p):
+        p = np.ascontiguousarray(p, np.float64)
+        assert p.shape == self.shape + (NP,), p.shape
+        _check(self.lib.hg_upload_prims(self.h, _ptr(p)), "hg_upload_prims")
+
+    def download(self):
+        p = np.empty(self.shape + (NP,))
+        _check(self.lib.hg_download_prims(self.h, _ptr(p)), "hg_download_prims")
+        return p
+
+    def set_time(self, t, dt):
+        _check(self.lib.hg_set_time(self.h, t, dt), "hg_set_time")
+
+    def step(self, n=1):
+        t = ctypes.c_double()
+        dt = ctypes.c_double()
+        _check(self.lib.hg_step(self.h, n, ctypes.byref(t), ctypes.byref(dt)), "hg_step")
+        return t.value, dt.value
+
+    def fail_counts(self):
+        v = np.zeros(NFAIL, np.uint64)
+        _check(self.lib.hg_get_fail_counts(self.h, _ptr(v)), "hg_get_fail_counts")
+        return v
+
+    def pflag(self):
+        v = np.empty(self.shape, np.int32)
+        _check(self.lib.hg_download_pflag(self.h, _ptr(v)), "hg_download_pflag")
+        return v
+
+    def gamma(self):
+        v = np.empty(self.shape)
+        _check(self.lib.hg_download_gamma(self.h, _ptr(v)), "hg_download_gamma")
+        return v
+
+    def nfail(self):
+        v = np.empty((NFAIL,) + self.shape, np.int32)
+        _check(self.lib.hg_download_nfail(self.h, _ptr(v)), "hg_download_nfail")
+        return v
+
+    def diag(self):
+        m = ctypes.c_double()
+        c = (ctypes.c_double * 3)()
+        _check(self.lib.hg_get_diag(self.h, ctypes.byref(m), c), "hg_get_diag")
+        return m.value, tuple(c)
+
+    def profile(self, enable=True):
+        _check(self.lib.hg_profile(self.h, 1 if enable else 0), "hg_profile")
+
+    def kernel_times(self):
+        """{class: (total ms, launches)} since the last profile() call."""
+        ms = np.zeros(len(KERNEL_CLASSES))
+        n = np.zeros(len(KERNEL_CLASSES), np.int64)
+        _check(self.lib.hg_kernel_times(self.h, _ptr(ms), _ptr(n)), "hg_kernel_times")
+        return {c: (float(ms[i]), int(n[i])) for i, c in enumerate(KERNEL_CLASSES)}
+
+    def last_step_ms(self):
+        v = ctypes.c_double()
+        _check(self.lib.hg_last_step_ms(self.h, ctypes.byref(v)), "hg_last_step_ms")
+        return v.value

@@ -1,0 +1,63 @@
+"""Build libharmgpu.so in-tree for sm_100a.
+
+nvcc flags: -gencode arch=compute_100a,code=sm_100a, -O3, -lineinfo, and
+-fmad=false: no multiply-add is fused, so every FP64 operation is rounded
+exactly as in the reference's gcc build and results agree bit for bit.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libharmgpu.so")
+SOURCES = ["hg_kernels.cu", "hg_api.cu"]
+HEADERS = ["hg_internal.h", "hg_phys.cuh", "hg_fallback.cuh"]
+
+
+def nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if c and (os.path.isabs(c) and os.path.exists(c) or not os.path.isabs(c)):
+            return c
+    return "nvcc"
+
+
+def flags():
+    return ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false", "-std=c++17",
+            "-Xcompiler", "-fPIC", "-I", os.path.join(REPO, "include"), "-I", CSRC]
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(REPO, "include", "harmgpu.h"), __file__]
+    return all(os.path.getmtime(d) <= t for d in deps)
+
+
+def build(force=False, verbose=False):
+    if not force and up_to_date():
+        return LIB
+    objs = []
+    procs = []
+    for s in SOURCES:
+        o = os.path.join(CSRC, s.replace(".cu", ".o"))
+        cmd = [nvcc()] + flags() + ["-c", os.path.join(CSRC, s), "-o", o]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((subprocess.Popen(cmd), s))
+        objs.append(o)
+    for p, s in procs:
+        if p.wait() != 0:
+            raise RuntimeError("nvcc failed on " + s)
+    tmp = LIB + ".tmp"
+    subprocess.check_call([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs)
+    os.replace(tmp, LIB)
+    for o in objs:
+        os.remove(o)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="-f" in sys.argv, verbose="-v" in sys.argv))

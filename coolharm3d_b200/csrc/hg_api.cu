@@ -1,0 +1,552 @@
+// hg_api.cu -- host side of libharmgpu: the C ABI declared in include/harmgpu.h.
+//
+// Owns the device-resident grid of one simulation, converts between the
+// reference's array layout (flattened p[i][j][k][l]) and the engine's
+// structure-of-arrays layout, and launches the step (hg_kernels.cu).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "harmgpu.h"
+#include "hg_internal.h"
+
+namespace hg {
+void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R);
+}  // namespace hg
+
+using hg::GridDev;
+
+struct hg_handle {
+  hg_grid_desc d;
+  GridDev G;
+  hg::LaunchCfg L;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  bool have_geom = false, have_cells = false, have_prims = false;
+  std::vector<void *> allocs;
+  double *h_stage = nullptr;  // pinned staging buffer, 8 planes
+  long ntot_ref = 0;          // N1TOT*N2TOT*N3TOT of the reference layout
+  int NT[3] = {0, 0, 0};      // reference extents
+  // per-kernel-class timing (hg_profile)
+  bool prof = false;
+  std::vector<cudaEvent_t> pev;
+  std::vector<int> pcls;
+  double kc_ms[hg::KC_N] = {0};
+  long long kc_n[hg::KC_N] = {0};
+};
+
+#define HG_CK(call)                                                                   \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      fprintf(stderr, "libharmgpu: %s failed: %s\n", #call, cudaGetErrorString(e_)); \
+      return HG_ERR_CUDA;                                                             \
+    }                                                                                 \
+  } while (0)
+
+// address of a field of the device-resident DevScalars (no host dereference)
+static void *sc_field(const GridDev &G, size_t off) { return (char *)G.sc + off; }
+
+static int dev_alloc(hg_handle *h, void **p, size_t bytes)
+{
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return HG_ERR_NOMEM;
+  }
+  cudaMemset(*p, 0, bytes);
+  h->allocs.push_back(*p);
+  return HG_OK;
+}
+
+extern "C" const char *hg_strerror(int code)
+{
+  switch (code) {
+    case HG_OK: return "ok";
+    case HG_ERR_CUDA: return "CUDA runtime error";
+    case HG_ERR_BADARG: return "invalid argument or unsupported switch value";
+    case HG_ERR_TIMEOUT: return "device-side wait timed out";
+    case HG_ERR_NOMEM: return "out of device memory";
+    case HG_ERR_STATE: return "call out of order";
+    case HG_ERR_DEVICE: return "kernel reported an internal error";
+    default: return "unknown error";
+  }
+}
+
+static int validate(const hg_grid_desc *d)
+{
+  if (!d) return HG_ERR_BADARG;
+  if (d->n1 < 1 || d->n2 < 1 || d->n3 < 1) return HG_ERR_BADARG;
+  if (d->n1 + 2 * HG_NGH >= (1 << 21) || d->n2 + 2 * HG_NGH >= (1 << 21) || d->n3 + 2 * HG_NGH >= (1 << 21))
+    return HG_ERR_BADARG;
+  if (d->recon_type < 0 || d->recon_type > 5) return HG_ERR_BADARG;
+  if (d->flux_type != 0 && d->flux_type != 1) return HG_ERR_BADARG;
+  if (d->bc_type != 0 && d->bc_type != 1) return HG_ERR_BADARG;
+  if (d->metric_dim != 0 && d->metric_dim != 2) return HG_ERR_BADARG;
+  if (d->cooling != 0) return HG_ERR_BADARG;
+  if (d->precision != HG_PREC_FP64) return HG_ERR_BADARG;
+  // the tables of METRIC_DIM 2 vary with i and j: those directions must be resolved
+  if (d->metric_dim == 2 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
+  if (d->rescale_r && d->n1 == 1) return HG_ERR_BADARG;
+  if (!(d->gam > 1.) || !(d->cour > 0.)) return HG_ERR_BADARG;
+  for (int a = 1; a < 4; a++)
+    if (!(d->dx[a] > 0.)) return HG_ERR_BADARG;
+  return HG_OK;
+}
+
+extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
+{
+  if (!out) return HG_ERR_BADARG;
+  *out = nullptr;
+  int rc = validate(desc);
+  if (rc) return rc;
+  HG_CK(cudaSetDevice(desc->device));
+  hg_handle *h = new (std::nothrow) hg_handle();
+  if (!h) return HG_ERR_NOMEM;
+  h->d = *desc;
+  GridDev &G = h->G;
+  memset(&G, 0, sizeof(G));
+  const int n[3] = {desc->n1, desc->n2, desc->n3};
+  long st = 1;
+  for (int a = 0; a < 3; a++) {
+    G.N[a] = n[a];
+    G.deg[a] = (n[a] == 1);
+    G.T[a] = G.deg[a] ? 1 : n[a] + 2 * HG_NGH;
+    G.NE[a] = n[a] + HG_NGH - 1;
+    h->NT[a] = n[a] + 2 * HG_NGH;
+  }
+  for (int a = 0; a < 3; a++) {
+    G.st[a] = G.deg[a] ? 0 : st;
+    st *= G.T[a];
+  }
+  G.S = st;
+  h->ntot_ref = (long)h->NT[0] * h->NT[1] * h->NT[2];
+  G.recon = desc->recon_type;
+  G.flux = desc->flux_type;
+  G.ct_para = desc->use_flux_ct_para;
+  G.bc = desc->bc_type;
+  G.mdim = desc->metric_dim;
+  G.use_ee = desc->use_entropy_eq;
+  G.cooling = desc->cooling;
+  G.rescale = desc->rescale_r;
+  G.nsd = (n[0] > 1) + (n[1] > 1) + (n[2] > 1);
+  G.gam = desc->gam;
+  G.cour = desc->cour;
+  for (int a = 0; a < 4; a++) {
+    G.dx[a] = desc->dx[a];
+    G.invdx[a] = 1. / desc->dx[a];
+    G.startx[a] = desc->startx[a];
+    G.grid_length[a] = desc->grid_length[a];
+  }
+  G.capacity = (long)n[0] * n[1] * n[2];
+  const size_t S8 = sizeof(double) * G.S;
+#define ALLOC(ptr, bytes)                                     \
+  do {                                                        \
+    void *q_ = nullptr;                                       \
+    if ((rc = dev_alloc(h, &q_, (bytes))) != HG_OK) goto fail; \
+    ptr = (decltype(ptr))q_;                                  \
+  } while (0)
+  {
+    ALLOC(G.p, S8 * HG_NPR);
+    ALLOC(G.ph, S8 * HG_NPR);
+    for (int d = 0; d < 3; d++) ALLOC(G.F[d], S8 * HG_NPR);
+    for (int d = 0; d < 3; d++) ALLOC(G.emf[d], S8);
+    ALLOC(G.p_gamma, S8);
+    ALLOC(G.pflag, sizeof(int) * G.S);
+    ALLOC(G.nfail, sizeof(unsigned int) * G.S * HG_NF);
+    ALLOC(G.floors, S8 * 2);
+    ALLOC(G.sc, sizeof(hg::DevScalars));
+    ALLOC(G.q_idx, sizeof(unsigned long long) * G.capacity);
+    ALLOC(G.q_U, sizeof(double) * HG_NPR * G.capacity);
+    ALLOC(G.fl_idx, sizeof(unsigned long long) * G.capacity);
+    if (G.mdim == 2) {
+      G.gS = (long)HG_NPOS * G.T[0] * G.T[1];
+      ALLOC(G.geomT, sizeof(double) * 42 * G.gS);
+      ALLOC(G.conn, sizeof(double) * 64 * G.T[0] * G.T[1]);
+    }
+    if (G.rescale) ALLOC(G.rsc, sizeof(double) * 12 * G.T[0]);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device);
+    auto grid_for = [&](long work, int per_sm) {
+      long g = (work + 127) / 128;
+      long cap = (long)sms * per_sm;
+      if (g > cap) g = cap;
+      if (g < 1) g = 1;
+      return (int)g;
+    };
+    long faces = (long)G.T[0] * G.T[1] * G.T[2];
+    h->L.grid_flux = grid_for(faces, 8);
+    h->L.grid_emf = grid_for(faces, 8);
+    h->L.grid_upd = grid_for(G.capacity, 8);
+    h->L.grid_fix = grid_for(G.capacity, 4);
+    h->L.grid_bnd = grid_for(faces - G.capacity, 8);
+    ALLOC(G.blk, sizeof(double) * h->L.grid_upd);
+    if (cudaMallocHost((void **)&h->h_stage, S8 * HG_NPR) != cudaSuccess) {
+      cudaGetLastError();
+      rc = HG_ERR_NOMEM;
+      goto fail;
+    }
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+      rc = HG_ERR_CUDA;
+      goto fail;
+    }
+    hg::DevScalars sc0;
+    memset(&sc0, 0, sizeof(sc0));
+    sc0.t = desc->t;
+    sc0.dt = desc->dx[0];
+    if (cudaMemcpy(G.sc, &sc0, sizeof(sc0), cudaMemcpyHostToDevice) != cudaSuccess) {
+      rc = HG_ERR_CUDA;
+      goto fail;
+    }
+  }
+#undef ALLOC
+  *out = h;
+  return HG_OK;
+fail:
+  hg_destroy(h);
+  return rc;
+}
+
+extern "C" void hg_destroy(hg_handle *h)
+{
+  if (!h) return;
+  cudaSetDevice(h->d.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
+  for (void *p : h->allocs) cudaFree(p);
+  if (h->h_stage) cudaFreeHost(h->h_stage);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+extern "C" int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom, const double *conn, int64_t n_conn)
+{
+  if (!h || !geom) return HG_ERR_BADARG;
+  GridDev &G = h->G;
+  HG_CK(cudaSetDevice(h->d.device));
+  if (G.mdim == 0) {
+    if (n_geom < 1) return HG_ERR_BADARG;
+    hg::Geom &g = G.g0;
+    memcpy(g.gcon, geom, 16 * 8);
+    memcpy(g.gcov, geom + 16, 16 * 8);
+    g.g = geom[32];
+    g.g_inv = geom[33];
+    g.alpha = geom[34];
+    for (int a = 0; a < 3; a++) g.beta[a] = geom[35 + a];
+    for (int a = 0; a < 4; a++) g.ncon[a] = geom[38 + a];
+  } else {
+    const int N1T = h->NT[0], N2T = h->NT[1];
+    if (n_geom != (int64_t)HG_NPOS * N1T * N2T || !conn || n_conn != (int64_t)G.N[0] * G.N[1]) return HG_ERR_BADARG;
+    std::vector<double> t((size_t)42 * G.gS);
+    for (int pos = 0; pos < HG_NPOS; pos++)
+      for (int i = 0; i < N1T; i++)
+        for (int j = 0; j < N2T; j++) {
+          const double *s = geom + 42L * (j + (long)N2T * (i + (long)N1T * pos));  // GEOM_ID
+          const long o = ((long)pos * G.T[1] + j) * G.T[0] + i;
+          for (int f = 0; f < 42; f++) t[f * G.gS + o] = s[f];
+        }
+    HG_CK(cudaMemcpy(G.geomT, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+    const long cS = (long)G.T[0] * G.T[1];
+    std::vector<double> c((size_t)64 * cS, 0.);
+    for (int i = 0; i < G.N[0]; i++)
+      for (int j = 0; j < G.N[1]; j++) {
+        const double *s = conn + 64L * (j + (long)G.N[1] * i);  // CONN_ID
+        const long o = (long)(j + HG_NGH) * G.T[0] + (i + HG_NGH);
+        for (int f = 0; f < 64; f++) c[f * cS + o] = s[f];
+      }
+    HG_CK(cudaMemcpy(G.conn, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+  }
+  h->have_geom = true;
+  return HG_OK;
+}
+
+// ref index of the stored zone along direction a for stored index x
+static inline int ref_of(const GridDev &G, int a, int x) { return G.deg[a] ? HG_NGH : x; }
+
+extern "C" int hg_set_cell_data(hg_handle *h, const double *cell6, const double *rface)
+{
+  if (!h || !cell6) return HG_ERR_BADARG;
+  GridDev &G = h->G;
+  HG_CK(cudaSetDevice(h->d.device));
+  const int N2T = h->NT[1], N3T = h->NT[2];
+  std::vector<double> fl((size_t)2 * G.S);
+  for (int k = 0; k < G.T[2]; k++)
+    for (int j = 0; j < G.T[1]; j++)
+      for (int i = 0; i < G.T[0]; i++) {
+        const long r = ((long)ref_of(G, 0, i) * N2T + ref_of(G, 1, j)) * N3T + ref_of(G, 2, k);
+        const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+        fl[o] = cell6[r * 6 + 0];
+        fl[G.S + o] = cell6[r * 6 + 1];
+      }
+  HG_CK(cudaMemcpy(G.floors, fl.data(), sizeof(double) * fl.size(), cudaMemcpyHostToDevice));
+  if (G.rescale) {
+    if (!rface) return HG_ERR_BADARG;
+    const int T0 = G.T[0];
+    std::vector<double> r((size_t)12 * T0);
+    for (int i = 0; i < T0; i++) {  // rescale_prims_r(), recon.c:1142-1165
+      double rloc = cell6[(((long)i * N2T + HG_NGH) * N3T + HG_NGH) * 6 + 2];
+      double rf2 = rloc * rloc;
+      r[0 * T0 + i] = sqrt(rf2 * rloc);
+      r[1 * T0 + i] = rf2 * rloc;
+      r[2 * T0 + i] = rloc;
+      rloc = rface[i];
+      rf2 = rloc * rloc;
+      r[3 * T0 + i] = sqrt(rf2 * rloc);
+      r[4 * T0 + i] = rf2 * rloc;
+      r[5 * T0 + i] = rloc;
+      for (int a = 0; a < 6; a++) r[(6 + a) * T0 + i] = 1 / r[a * T0 + i];
+    }
+    HG_CK(cudaMemcpy(G.rsc, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice));
+  }
+  h->have_cells = true;
+  return HG_OK;
+}
+
+template <class GET>
+static int upload_impl(hg_handle *h, GET get)
+{
+  GridDev &G = h->G;
+  HG_CK(cudaSetDevice(h->d.device));
+  double *st = h->h_stage;
+  for (int k = 0; k < G.T[2]; k++)
+    for (int j = 0; j < G.T[1]; j++)
+      for (int i = 0; i < G.T[0]; i++) {
+        const double *src = get(ref_of(G, 0, i), ref_of(G, 1, j), ref_of(G, 2, k));
+        const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+        for (int l = 0; l < HG_NPR; l++) st[l * G.S + o] = src[l];
+      }
+  HG_CK(cudaMemcpyAsync(G.p, st, sizeof(double) * HG_NPR * G.S, cudaMemcpyHostToDevice, h->stream));
+  HG_CK(cudaMemsetAsync(G.nfail, 0, sizeof(unsigned int) * HG_NF * G.S, h->stream));
+  HG_CK(cudaMemsetAsync(G.pflag, 0, sizeof(int) * G.S, h->stream));
+  HG_CK(cudaMemsetAsync(sc_field(G, offsetof(hg::DevScalars, nfailtot)), 0, sizeof(unsigned long long) * 16, h->stream));
+  HG_CK(cudaStreamSynchronize(h->stream));
+  h->have_prims = true;
+  return HG_OK;
+}
+
+template <class PUT>
+static int download_impl(hg_handle *h, PUT put)
+{
+  GridDev &G = h->G;
+  HG_CK(cudaSetDevice(h->d.device));
+  double *st = h->h_stage;
+  HG_CK(cudaMemcpyAsync(st, G.p, sizeof(double) * HG_NPR * G.S, cudaMemcpyDeviceToHost, h->stream));
+  HG_CK(cudaStreamSynchronize(h->stream));
+  for (int i = 0; i < h->NT[0]; i++)
+    for (int j = 0; j < h->NT[1]; j++)
+      for (int k = 0; k < h->NT[2]; k++) {
+        double *dst = put(i, j, k);
+        const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+        for (int l = 0; l < HG_NPR; l++) dst[l] = st[l * G.S + o];
+      }
+  return HG_OK;
+}
+
+extern "C" int hg_upload_prims(hg_handle *h, const double *p)
+{
+  if (!h || !p) return HG_ERR_BADARG;
+  const int N2T = h->NT[1], N3T = h->NT[2];
+  return upload_impl(h, [&](int i, int j, int k) { return p + (((long)i * N2T + j) * N3T + k) * HG_NPR; });
+}
+
+extern "C" int hg_download_prims(hg_handle *h, double *p)
+{
+  if (!h || !p) return HG_ERR_BADARG;
+  const int N2T = h->NT[1], N3T = h->NT[2];
+  return download_impl(h, [&](int i, int j, int k) { return p + (((long)i * N2T + j) * N3T + k) * HG_NPR; });
+}
+
+extern "C" int hg_upload_prims_tree(hg_handle *h, double ****p)
+{
+  if (!h || !p) return HG_ERR_BADARG;
+  return upload_impl(h, [&](int i, int j, int k) { return (const double *)p[i][j][k]; });
+}
+
+extern "C" int hg_download_prims_tree(hg_handle *h, double ****p)
+{
+  if (!h || !p) return HG_ERR_BADARG;
+  return download_impl(h, [&](int i, int j, int k) { return p[i][j][k]; });
+}
+
+extern "C" int hg_set_time(hg_handle *h, double t, double dt)
+{
+  if (!h) return HG_ERR_BADARG;
+  HG_CK(cudaSetDevice(h->d.device));
+  double v[2] = {t, dt};
+  HG_CK(cudaMemcpy(sc_field(h->G, offsetof(hg::DevScalars, t)), v, sizeof(v), cudaMemcpyHostToDevice));
+  return HG_OK;
+}
+
+extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
+{
+  if (!h || nsteps < 0) return HG_ERR_BADARG;
+  if (!h->have_geom || !h->have_cells || !h->have_prims) return HG_ERR_STATE;
+  HG_CK(cudaSetDevice(h->d.device));
+  hg::EventRec rec, *R = nullptr;
+  if (h->prof) {
+    const size_t need = (size_t)40 * (nsteps > 0 ? nsteps : 1);
+    while (h->pev.size() < need) {
+      cudaEvent_t e;
+      HG_CK(cudaEventCreate(&e));
+      h->pev.push_back(e);
+    }
+    h->pcls.resize(h->pev.size());
+    rec.ev = (void **)h->pev.data();
+    rec.cls = h->pcls.data();
+    rec.n = 0;
+    rec.cap = (int)h->pev.size();
+    R = &rec;
+  }
+  HG_CK(cudaEventRecord(h->ev0, h->stream));
+  for (int s = 0; s < nsteps; s++) hg::launch_step(h->G, h->L, h->stream, R);
+  HG_CK(cudaGetLastError());
+  HG_CK(cudaEventRecord(h->ev1, h->stream));
+  HG_CK(cudaEventSynchronize(h->ev1));
+  HG_CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+  if (R) {
+    for (int e = 0; e + 1 < R->n; e++) {
+      float ms = 0.f;
+      HG_CK(cudaEventElapsedTime(&ms, h->pev[e], h->pev[e + 1]));
+      const int c = R->cls[e];
+      if (c >= 0 && c < hg::KC_END) {
+        h->kc_ms[c] += ms;
+        h->kc_n[c] += 1;
+      }
+    }
+  }
+  hg::DevScalars sc;
+  HG_CK(cudaMemcpy(&sc, h->G.sc, sizeof(sc), cudaMemcpyDeviceToHost));
+  if (sc.err) return HG_ERR_DEVICE;
+  if (t) *t = sc.t;
+  if (dt) *dt = sc.dt;
+  return HG_OK;
+}
+
+extern "C" int hg_get_fail_counts(hg_handle *h, uint64_t nfailtot[HG_NFAIL])
+{
+  if (!h || !nfailtot) return HG_ERR_BADARG;
+  HG_CK(cudaSetDevice(h->d.device));
+  unsigned long long v[16];
+  HG_CK(cudaMemcpy(v, sc_field(h->G, offsetof(hg::DevScalars, nfailtot)), sizeof(v), cudaMemcpyDeviceToHost));
+  for (int l = 0; l < HG_NFAIL; l++) nfailtot[l] = v[l];
+  return HG_OK;
+}
+
+template <class T>
+static int download_cellwise(hg_handle *h, const T *dsrc, T *out, int planes)
+{
+  GridDev &G = h->G;
+  HG_CK(cudaSetDevice(h->d.device));
+  std::vector<T> tmp((size_t)planes * G.S);
+  HG_CK(cudaMemcpy(tmp.data(), dsrc, sizeof(T) * tmp.size(), cudaMemcpyDeviceToHost));
+  const long nref = h->ntot_ref;
+  for (int pl = 0; pl < planes; pl++)
+    for (int i = 0; i < h->NT[0]; i++)
+      for (int j = 0; j < h->NT[1]; j++)
+        for (int k = 0; k < h->NT[2]; k++) {
+          const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+          out[pl * nref + ((long)i * h->NT[1] + j) * h->NT[2] + k] = tmp[pl * G.S + o];
+        }
+  return HG_OK;
+}
+
+extern "C" int hg_download_pflag(hg_handle *h, int32_t *pflag)
+{
+  if (!h || !pflag) return HG_ERR_BADARG;
+  return download_cellwise<int>(h, h->G.pflag, pflag, 1);
+}
+
+extern "C" int hg_download_gamma(hg_handle *h, double *g)
+{
+  if (!h || !g) return HG_ERR_BADARG;
+  return download_cellwise<double>(h, h->G.p_gamma, g, 1);
+}
+
+extern "C" int hg_download_nfail(hg_handle *h, int32_t *nfail)
+{
+  if (!h || !nfail) return HG_ERR_BADARG;
+  return download_cellwise<int>(h, (const int *)h->G.nfail, nfail, HG_NF);
+}
+
+extern "C" int hg_get_diag(hg_handle *h, double *m_tot, double mcs[3])
+{
+  if (!h) return HG_ERR_BADARG;
+  HG_CK(cudaSetDevice(h->d.device));
+  hg::DevScalars sc;
+  HG_CK(cudaMemcpy(&sc, h->G.sc, sizeof(sc), cudaMemcpyDeviceToHost));
+  if (m_tot) *m_tot = sc.m_tot;
+  if (mcs)
+    for (int a = 0; a < 3; a++) mcs[a] = sc.last_maxs[a + 1];
+  return HG_OK;
+}
+
+extern "C" int hg_profile(hg_handle *h, int32_t enable)
+{
+  if (!h) return HG_ERR_BADARG;
+  h->prof = enable != 0;
+  for (int c = 0; c < hg::KC_N; c++) {
+    h->kc_ms[c] = 0.;
+    h->kc_n[c] = 0;
+  }
+  return HG_OK;
+}
+
+extern "C" int hg_kernel_times(hg_handle *h, double ms[HG_NKCLASS], int64_t launches[HG_NKCLASS])
+{
+  if (!h || !ms || !launches) return HG_ERR_BADARG;
+  for (int c = 0; c < HG_NKCLASS; c++) {
+    ms[c] = h->kc_ms[c];
+    launches[c] = h->kc_n[c];
+  }
+  return HG_OK;
+}
+
+extern "C" int hg_last_step_ms(hg_handle *h, double *ms)
+{
+  if (!h || !ms) return HG_ERR_BADARG;
+  *ms = h->last_ms;
+  return HG_OK;
+}
+
+// calc_all_geom() for METRIC_MINK_CARTESIAN / COORD_IDENTITY (metric.c:4130-4140,
+// 4235-4247) and coord_of_xp()'s floors (coord.c:3775-3796, FLOOR_STATIC).
+extern "C" int hg_build_geometry_minkowski(const hg_grid_desc *d, double *geom, double *cell6)
+{
+  if (!d || !geom || !cell6) return HG_ERR_BADARG;
+  for (int f = 0; f < 42; f++) geom[f] = 0.;
+  geom[0] = -1.; geom[5] = 1.; geom[10] = 1.; geom[15] = 1.;           // gcon
+  geom[16] = -1.; geom[21] = 1.; geom[26] = 1.; geom[31] = 1.;         // gcov
+  geom[32] = 1.;                                                       // g
+  geom[33] = 1. / geom[32];                                            // g_inv
+  geom[38] = sqrt(-geom[0]);                                           // ncon[0] = 1/alpha
+  geom[34] = 1. / geom[38];                                            // alpha
+  for (int a = 1; a < 4; a++) geom[38 + a] = -geom[34] * geom[a];      // ncon[1..3]
+  for (int a = 0; a < 3; a++) geom[35 + a] = -geom[a + 1] / geom[0];   // beta
+  const double RHOMIN = 2.e-10, UUMIN = 2.e-12, RHOPOWER = -1.5, UUPOWER = -2.5;
+  const int N1T = d->n1 + 6, N2T = d->n2 + 6, N3T = d->n3 + 6;
+  for (int i = 0; i < N1T; i++)
+    for (int j = 0; j < N2T; j++)
+      for (int k = 0; k < N3T; k++) {
+        const double x1 = d->startx[1] + (i + 0.5) * d->dx[1];
+        const double x2 = d->startx[2] + (j + 0.5) * d->dx[2];
+        const double x3 = d->startx[3] + (k + 0.5) * d->dx[3];
+        const double r = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+        double *c = cell6 + (((long)i * N2T + j) * N3T + k) * 6;
+        c[0] = RHOMIN * pow(r, RHOPOWER);
+        c[1] = UUMIN * pow(r, UUPOWER);
+        c[2] = r;
+        c[3] = x1;
+        c[4] = x2;
+        c[5] = x3;
+      }
+  return HG_OK;
+}

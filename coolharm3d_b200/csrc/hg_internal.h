@@ -1,0 +1,111 @@
+// hg_internal.h -- shared definitions of the libharmgpu engine (host + device).
+//
+// Device layout (HBM): structure of arrays.  Every grid function is stored as
+// planes of T0*T1*T2 doubles, x1 (index i) fastest, so warps that map lanes to
+// consecutive i read coalesced 256-byte segments for stencils along any of the
+// three directions.  A direction with a single physical zone (N == 1) is
+// "degenerate": the reference keeps NG ghost copies of that zone (recon.c:
+// 1050-1075, bounds.c), which are bit-identical to the zone itself, so here it
+// is stored once (T = 1, stride 0) and every index along it maps to that zone.
+// Indices used in kernels are the reference's own (ghost-inclusive, 0..N+5).
+#pragma once
+#include <cstdint>
+
+#define HG_NPR 8
+#define HG_NGH 3
+#define HG_NF 15
+#define HG_NPOS 5
+
+namespace hg {
+
+enum { RHO = 0, UU, U1, U2, U3, B1, B2, B3 };
+
+// nfail[] slots (macros.h:243-258)
+enum { NF_FLOOR = 0, NF_TMAX, NF_GAMMA_MAX, NF_GAMMA_CALC, NF_USE_FULL_INV, NF_USE_EE, NF_UTOPRIM,
+       NF_UTOPRIM_EE, NF_USE_INTERP_PRIM, NF_USE_INTERP_V, NF_INTERP_PRIM, NF_INTERP_V };
+enum { PF_NONE = 0, PF_INTERP_V = 1, PF_INTERP_PRIM = 2 };
+
+struct Geom {
+  double gcon[4][4];
+  double gcov[4][4];
+  double g, g_inv, alpha;
+  double beta[3];
+  double ncon[4];
+};
+
+// Device-resident scalars of one grid (t, dx[0], reductions, failure flags).
+struct DevScalars {
+  double t, dt;
+  unsigned long long maxs[4];       // bit patterns of max_char_speed[1..3] (non-negative doubles)
+  unsigned long long nfailtot[16];  // nfailtot[N_NFAIL]
+  int failure_exists;
+  int ftype[3];                     // failure_type[N_PFLAG_TYPES]
+  int bnd_phys;                     // boundary_phys_pflag
+  int q_count;                      // cells queued for the inversion fallback tree
+  int fl_count;                     // cells flagged for interpolation
+  int err;                          // internal error status (queue overflow ...)
+  double m_tot;
+  double last_maxs[4];              // max_char_speed of the last corrector, as doubles
+};
+
+// Everything a kernel needs, passed by value.
+struct GridDev {
+  int N[3];          // physical zones
+  int T[3];          // stored extent per direction (N+6, or 1 when degenerate)
+  int deg[3];        // 1 if N == 1
+  long st[3];        // stride per direction (0 when degenerate)
+  long S;            // plane size
+  int NE[3];         // last physical index N+2
+  int recon, flux, ct_para, bc, mdim, use_ee, cooling, rescale, nsd;
+  double gam, cour;
+  double dx[4], invdx[4];
+  double startx[4], grid_length[4];
+  // state
+  double *p, *ph;            // 8 planes each
+  double *F[3];              // 8 planes each, face index = lower face of the cell
+  double *emf[3];            // corner EMFs
+  double *p_gamma;
+  int *pflag;
+  unsigned int *nfail;       // HG_NF planes
+  double *floors;            // 2 planes: rhoflr, uuflr
+  double *geomT;             // metric_dim 2: 42 planes of HG_NPOS*T0*T1, index (pos*T1 + j)*T0 + i
+  long gS;                   // geometry plane size
+  double *conn;              // metric_dim 2: 64 planes of T0*T1 (physical i,j only used)
+  double *rsc;               // RESCALE_R: 9 planes of T0: rscale[0..5], and 1/rscale[0..2]
+  DevScalars *sc;
+  unsigned long long *q_idx; // fallback queue: packed (i,j,k)
+  double *q_U;               // 8 doubles per queued cell
+  unsigned long long *fl_idx;// interpolation list: packed (i,j,k)
+  long capacity;             // N0*N1*N2
+  double *blk;               // per-block partial sums of M_tot
+  Geom g0;                   // metric_dim 0 geometry
+};
+
+// Fixed grid sizes of the step's kernels (grid-stride loops).
+struct LaunchCfg {
+  int grid_flux, grid_emf, grid_upd, grid_fix, grid_bnd;
+};
+
+// Kernel classes timed by the optional event recorder.
+enum { KC_FLUX = 0, KC_EMF, KC_UPDATE, KC_FALLBACK, KC_BOUNDS, KC_FIXUP, KC_MISC, KC_END, KC_N };
+
+// Optional CUDA-event recorder: an event is recorded on the launch stream
+// before every kernel (tagged with its class) and one after the last.
+struct EventRec {
+  void **ev;   // cudaEvent_t pool
+  int *cls;
+  int n, cap;
+};
+
+__host__ __device__ inline unsigned long long pack_ijk(int i, int j, int k)
+{
+  return (unsigned long long)i | ((unsigned long long)j << 21) | ((unsigned long long)k << 42);
+}
+__host__ __device__ inline void unpack_ijk(unsigned long long v, int &i, int &j, int &k)
+{
+  i = (int)(v & 0x1FFFFF);
+  j = (int)((v >> 21) & 0x1FFFFF);
+  k = (int)((v >> 42) & 0x1FFFFF);
+}
+
+}  // namespace hg

@@ -1,0 +1,889 @@
+// hg_kernels.cu -- sm_100a kernels of one HARM3D time step (step_ch.c:50-234).
+//
+// Per substep (predictor with Dt/2, corrector with Dt):
+//   k_begin     reset the substep's reductions and failure flags
+//   k_flux x3   one kernel per direction: reconstruction of the six-zone
+//               stencil of each face (reconstruct_fast, recon.c:894-1103)
+//               fused with get_state/primtoflux/vchar_fast and the HLL or LF
+//               flux (numerical_flux, step_ch.c:636-790); the maximum
+//               characteristic speed is reduced per block into one atomic
+//   k_emf       corner EMFs of flux_ct_para_fast2 / flux_ct (flux_ct.c)
+//   k_update    conserved update with the geometric source and the CT
+//               corrected induction fluxes, then the 2D Newton inversion
+//               (advance, step_ch.c:312-399); zones that need the rest of
+//               the recover_primitives() tree are queued
+//   k_fallback  Utoprim_1d / entropy fix / floors for the queued zones
+//   k_bounds    ghost zones (bounds.c) and pflag ghosts
+//   k_fixup     fixup_interp_v / fixup_interp_prim over the flagged zones
+//   k_bounds    again if a flagged zone touched a physical boundary
+// then k_timestep (timestep(), step_ch.c:546-623) on one block.
+// All loops are grid-stride loops over a fixed grid so that reductions are
+// per block and deterministic.
+#include <cuda_runtime.h>
+
+#include "hg_fallback.cuh"
+
+namespace hg {
+
+#define HG_BLK 128
+
+__device__ __forceinline__ int rs_type(int l) { return l == RHO ? 0 : (l == UU ? 2 : 1); }
+
+// (x * rscale) * (1/rscale): the value rescale_prims_r() leaves in p_h after
+// it scaled and unscaled it around the x1 reconstruction (recon.c:1168-1200).
+__device__ __forceinline__ double rs_roundtrip(const GridDev &G, double x, int l, int i)
+{
+  const int t = rs_type(l);
+  return (x * G.rsc[t * G.T[0] + i]) * G.rsc[(6 + t) * G.T[0] + i];
+}
+
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *dst)
+{
+  __shared__ double red[HG_BLK / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double w = __shfl_down_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = red[0];
+    for (int w = 1; w < HG_BLK / 32; w++) m = red[w] > m ? red[w] : m;
+    if (m > 0.) atomicMax(dst, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v)
+{
+  __shared__ double red[HG_BLK / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < HG_BLK / 32; w++) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+__device__ __forceinline__ unsigned int block_count(unsigned int v)
+{
+  __shared__ unsigned int red[HG_BLK / 32];
+  v = __reduce_add_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  unsigned int s = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < HG_BLK / 32; w++) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+// fail() bookkeeping (diag.c:159-330) for the rare branches: per-zone nfail
+// counter and the global total, both atomic.
+__device__ __forceinline__ void book(const GridDev &G, int nf, int i, int j, int k)
+{
+  atomicAdd(&G.nfail[nf * G.S + off3(G, i, j, k)], 1u);
+  atomicAdd(&G.sc->nfailtot[nf], 1ull);
+}
+
+// FAIL_GAMMA_CALC at a face: the reference computes each face once per ghost
+// copy of a degenerate direction (numerical_flux's ranges), booking it once
+// per copy; mult is that number of copies.
+__device__ __forceinline__ void book_face(const GridDev &G, int i, int j, int k, unsigned int mult)
+{
+  atomicAdd(&G.nfail[NF_GAMMA_CALC * G.S + off3(G, i, j, k)], mult);
+  atomicAdd(&G.sc->nfailtot[NF_GAMMA_CALC], (unsigned long long)mult);
+}
+
+// fail(type, state != 0): pflag, failure flags, boundary flag
+// (check_boundary_pflag, harm_mpi.c:1388-1426) and the interpolation list.
+__device__ __forceinline__ void flag_zone(const GridDev &G, int pf, int i, int j, int k)
+{
+  G.pflag[off3(G, i, j, k)] = pf;
+  G.sc->failure_exists = 1;
+  G.sc->ftype[pf] = 1;
+  const int n0 = G.N[0] + HG_NGH - 1, n1 = G.N[1] + HG_NGH - 1, n2 = G.N[2] + HG_NGH - 1;
+  if (i < 2 * HG_NGH || i > n0 - HG_NGH || j < 2 * HG_NGH || j > n1 - HG_NGH || k < 2 * HG_NGH || k > n2 - HG_NGH)
+    G.sc->bnd_phys = 1;
+  const int slot = atomicAdd(&G.sc->fl_count, 1);
+  if (slot < G.capacity) G.fl_idx[slot] = pack_ijk(i, j, k);
+  else G.sc->err = 1;
+}
+
+// Left/right primitive states of face (i,j,k) in direction d (p_L[i][j][k][d],
+// p_R[i][j][k][d] of reconstruct_fast).
+template <bool RS>
+__device__ __forceinline__ void face_prims(const GridDev &G, const double *__restrict__ ph, int d, int i, int j,
+                                           int k, double *pl, double *pr)
+{
+  const long o = off3(G, i, j, k);
+  if (G.deg[d]) {
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) {
+      double v = __ldg(ph + l * G.S + o);
+      if (RS) v = rs_roundtrip(G, v, l, i);
+      pl[l] = pr[l] = v;
+    }
+    return;
+  }
+  const long st = G.st[d];
+#pragma unroll
+  for (int l = 0; l < HG_NPR; l++) {
+    double y[6];
+    const double *b = ph + l * G.S + o - 3 * st;
+#pragma unroll
+    for (int m = 0; m < 6; m++) y[m] = __ldg(b + m * st);
+    if (RS) {
+      const int t = rs_type(l);
+      if (d == 0) {
+#pragma unroll
+        for (int m = 0; m < 6; m++) y[m] *= G.rsc[t * G.T[0] + i - 3 + m];
+      } else {
+#pragma unroll
+        for (int m = 0; m < 6; m++) y[m] = rs_roundtrip(G, y[m], l, i);
+      }
+    }
+    recon_face(G.recon, y, &pl[l], &pr[l]);
+    if (RS && d == 0) {
+      const double f = G.rsc[(9 + rs_type(l)) * G.T[0] + i];
+      pl[l] *= f;
+      pr[l] *= f;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_flux: F[d] on faces [lo, lo+n) (reference indices).
+template <bool RS>
+__global__ void __launch_bounds__(HG_BLK) k_flux(GridDev G, const double *__restrict__ ph, int d, int lo0, int lo1,
+                                                 int lo2, int n0, int n1, int n2, unsigned int mult)
+{
+  const long total = (long)n0 * n1 * n2;
+  const int dim = d + 1;
+  double *__restrict__ Fd = G.F[d];
+  double vmax = 0.;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = lo0 + (int)(t % n0);
+    const int j = lo1 + (int)((t / n0) % n1);
+    const int k = lo2 + (int)(t / ((long)n0 * n1));
+    double pl[HG_NPR], pr[HG_NPR];
+    face_prims<RS>(G, ph, d, i, j, k, pl, pr);
+    Geom g;
+    load_geom(G, d, i, j, g);
+    State ql, qr;
+    if (get_state(pl, g, G.gam, ql)) book_face(G, i, j, k, mult);
+    if (get_state(pr, g, G.gam, qr)) book_face(G, i, j, k, mult);
+    double Ul[HG_NPR], Ur[HG_NPR], Fl[HG_NPR], Fr[HG_NPR];
+    primtoflux(pl, ql, 0, g, Ul);
+    primtoflux(pr, qr, 0, g, Ur);
+    primtoflux(pl, ql, dim, g, Fl);
+    primtoflux(pr, qr, dim, g, Fr);
+    double cmaxl, cminl, cmaxr, cminr;
+    vchar_fast(ql, g, dim, G.gam, &cmaxl, &cminl);
+    vchar_fast(qr, g, dim, G.gam, &cmaxr, &cminr);
+    const double a0 = 0. > cmaxl ? 0. : cmaxl;
+    const double cmax = fabs(a0 > cmaxr ? a0 : cmaxr);
+    const double a1 = 0. > -cminl ? 0. : -cminl;
+    const double cmin = fabs(a1 > -cminr ? a1 : -cminr);
+    const double ctop = cmin > cmax ? cmin : cmax;
+    if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
+      if (ctop > vmax) vmax = ctop;
+    const long o = off3(G, i, j, k);
+    if (G.flux == 1) {
+      const double den = cmax + cmin + HG_SMALL;
+#pragma unroll
+      for (int l = 0; l < HG_NPR; l++) Fd[l * G.S + o] = (cmax * Fl[l] + cmin * Fr[l] - cmax * cmin * (Ur[l] - Ul[l])) / den;
+    } else {
+#pragma unroll
+      for (int l = 0; l < HG_NPR; l++) Fd[l * G.S + o] = 0.5 * (Fl[l] + Fr[l] - ctop * (Ur[l] - Ul[l]));
+    }
+  }
+  block_max_atomic(vmax, &G.sc->maxs[dim]);
+}
+
+// ---------------------------------------------------------------------------
+// k_emf: corner EMFs at [lo, lo+n).
+// Right edge of zone c-1 and left edge of zone c on a line through the corner
+// (flux_ct.c:782-900 accumulate exactly these two into each corner).
+__device__ __forceinline__ void line_edges(const GridDev &G, const double *__restrict__ f, long o, int a, double *rprev,
+                                           double *lcur)
+{
+  if (G.deg[a]) {
+    *rprev = *lcur = __ldg(f + o);
+    return;
+  }
+  const long st = G.st[a];
+  double y[6];
+#pragma unroll
+  for (int m = 0; m < 6; m++) y[m] = __ldg(f + o + (m - 3) * st);
+  ppm_face(G.recon, y, rprev, lcur);
+}
+
+__global__ void __launch_bounds__(HG_BLK) k_emf(GridDev G, int lo0, int lo1, int lo2, int n0, int n1, int n2)
+{
+  const long total = (long)n0 * n1 * n2;
+  const double *F0 = G.F[0], *F1 = G.F[1], *F2 = G.F[2];
+  const long S = G.S;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = lo0 + (int)(t % n0);
+    const int j = lo1 + (int)((t / n0) % n1);
+    const int k = lo2 + (int)(t / ((long)n0 * n1));
+    const long o = off3(G, i, j, k);
+    double e0, e1, e2;
+    if (G.ct_para) {
+      double r, l, r2, l2;
+      line_edges(G, F1 + B3 * S, o, 2, &r, &l);
+      line_edges(G, F2 + B2 * S, o, 1, &r2, &l2);
+      e0 = (((0. + r) + l) - r2) - l2;
+      line_edges(G, F2 + B1 * S, o, 0, &r, &l);
+      line_edges(G, F0 + B3 * S, o, 2, &r2, &l2);
+      e1 = (((0. + r) + l) - r2) - l2;
+      line_edges(G, F0 + B2 * S, o, 1, &r, &l);
+      line_edges(G, F1 + B1 * S, o, 0, &r2, &l2);
+      e2 = (((0. + r) + l) - r2) - l2;
+    } else {  // flux_ct.c:33-41
+      const long oi = off3(G, i - 1, j, k), oj = off3(G, i, j - 1, k), ok = off3(G, i, j, k - 1);
+      e0 = 0.25 * (F1[B3 * S + o] + F1[B3 * S + ok] - F2[B2 * S + o] - F2[B2 * S + oj]);
+      e1 = 0.25 * (F2[B1 * S + o] + F2[B1 * S + oi] - F0[B3 * S + o] - F0[B3 * S + ok]);
+      e2 = 0.25 * (F0[B2 * S + o] + F0[B2 * S + oj] - F1[B1 * S + o] - F1[B1 * S + oi]);
+    }
+    G.emf[0][o] = e0;
+    G.emf[1][o] = e1;
+    G.emf[2][o] = e2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// source(), phys.c:121-187 (cooling off): T^mu_kappa Gamma^kappa_nu mu for
+// METRIC_DIM 2 (U1, U2 only), times sqrt(-g).  Returns 1 on a gamma failure.
+__device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, const Geom &g, int i, int j, double *dU)
+{
+#pragma unroll
+  for (int l = 0; l < HG_NPR; l++) dU[l] = 0.;
+  int bad = 0;
+  if (G.mdim > 0) {
+    State q;
+    bad = get_state(ph, g, G.gam, q);
+    double mhd[4][4];
+    mhd_row(q, 0, mhd[0]);
+    mhd_row(q, 1, mhd[1]);
+    mhd_row(q, 2, mhd[2]);
+    mhd_row(q, 3, mhd[3]);
+    const long cS = (long)G.T[0] * G.T[1];
+    const long co = (long)(G.deg[1] ? 0 : j) * G.T[0] + (G.deg[0] ? 0 : i);
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        dU[U1] += mhd[a][b] * __ldg(G.conn + ((b * 4 + 1) * 4 + a) * cS + co);
+        dU[U2] += mhd[a][b] * __ldg(G.conn + ((b * 4 + 2) * 4 + a) * cS + co);
+      }
+  }
+  dU[UU] *= g.g;
+  dU[U1] *= g.g;
+  dU[U2] *= g.g;
+  dU[U3] *= g.g;
+  return bad;
+}
+
+// Conserved update of one zone (step_ch.c:320-370).
+__device__ __forceinline__ void update_zone(const GridDev &G, int i, int j, int k, double Dt, const double *dU, double *U)
+{
+  const long S = G.S, o = off3(G, i, j, k);
+  const long oi = o + G.st[0], oj = o + G.st[1], ok = o + G.st[2];
+  const double *F0 = G.F[0], *F1 = G.F[1], *F2 = G.F[2];
+#pragma unroll
+  for (int l = 0; l < B1; l++) {
+    const double a = F0[l * S + oi] - F0[l * S + o];
+    const double b = F1[l * S + oj] - F1[l * S + o];
+    const double c = F2[l * S + ok] - F2[l * S + o];
+    U[l] += Dt * (-(a)*G.invdx[1] - (b)*G.invdx[2] - (c)*G.invdx[3] + dU[l]);
+  }
+  // induction fluxes after flux_ct: zeroed, then + fac * (sum of two EMFs)
+  const double fac = G.ct_para ? 0.125 : 0.5;
+  const double *E0 = G.emf[0], *E1 = G.emf[1], *E2 = G.emf[2];
+  const long oij = o + G.st[0] + G.st[1], oik = o + G.st[0] + G.st[2], ojk = o + G.st[1] + G.st[2];
+  // x1 faces
+  const double f0b2_m = 0. + fac * (E2[o] + E2[oj]);
+  const double f0b2_p = 0. + fac * (E2[oi] + E2[oij]);
+  const double f0b3_m = 0. + (-fac) * (E1[o] + E1[ok]);
+  const double f0b3_p = 0. + (-fac) * (E1[oi] + E1[oik]);
+  // x2 faces
+  const double f1b1_m = 0. + (-fac) * (E2[o] + E2[oi]);
+  const double f1b1_p = 0. + (-fac) * (E2[oj] + E2[oij]);
+  const double f1b3_m = 0. + fac * (E0[o] + E0[ok]);
+  const double f1b3_p = 0. + fac * (E0[oj] + E0[ojk]);
+  // x3 faces
+  const double f2b1_m = 0. + fac * (E1[o] + E1[oi]);
+  const double f2b1_p = 0. + fac * (E1[ok] + E1[oik]);
+  const double f2b2_m = 0. + (-fac) * (E0[o] + E0[oj]);
+  const double f2b2_p = 0. + (-fac) * (E0[ok] + E0[ojk]);
+  const double zero = 0.;
+  U[B1] += Dt * (-(zero - zero) * G.invdx[1] - (f1b1_p - f1b1_m) * G.invdx[2] - (f2b1_p - f2b1_m) * G.invdx[3] + dU[B1]);
+  U[B2] += Dt * (-(f0b2_p - f0b2_m) * G.invdx[1] - (zero - zero) * G.invdx[2] - (f2b2_p - f2b2_m) * G.invdx[3] + dU[B2]);
+  U[B3] += Dt * (-(f0b3_p - f0b3_m) * G.invdx[1] - (f1b3_p - f1b3_m) * G.invdx[2] - (zero - zero) * G.invdx[3] + dU[B3]);
+}
+
+// k_update: every physical zone.  sub = 0 predictor (p_f = ph), 1 corrector (p_f = p).
+template <bool RS>
+__global__ void __launch_bounds__(HG_BLK) k_update(GridDev G, int sub, double dtfac, const double *__restrict__ p_h,
+                                                   double *__restrict__ p_f)
+{
+  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
+  const long total = (long)N0 * N1 * N2;
+  const double Dt = dtfac * G.sc->dt;
+  const long S = G.S;
+  const double *p = G.p;
+  double msum = 0.;
+  unsigned int n_full = 0, n_floor = 0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = HG_NGH + (int)(t % N0);
+    const int j = HG_NGH + (int)((t / N0) % N1);
+    const int k = HG_NGH + (int)(t / ((long)N0 * N1));
+    const long o = off3(G, i, j, k);
+    Geom g;
+    load_geom(G, 3, i, j, g);
+    double pi[HG_NPR], U[HG_NPR], dU[HG_NPR], pg[HG_NPR];
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) {
+      pg[l] = p[l * S + o];
+      pi[l] = RS ? rs_roundtrip(G, pg[l], l, i) : pg[l];
+    }
+    {  // U(p_i) at the start of the step (U_gf[0])
+      State q;
+      if (get_state(pi, g, G.gam, q) && sub == 0) book(G, NF_GAMMA_CALC, i, j, k);
+      primtoflux(pi, q, 0, g, U);
+    }
+    if (sub == 0) {
+      if (source_terms(G, pi, g, i, j, dU)) book(G, NF_GAMMA_CALC, i, j, k);
+    } else {
+      double phv[HG_NPR];
+#pragma unroll
+      for (int l = 0; l < HG_NPR; l++) {
+        const double v = p_h[l * S + o];
+        phv[l] = RS ? rs_roundtrip(G, v, l, i) : v;
+      }
+      if (source_terms(G, phv, g, i, j, dU)) book(G, NF_GAMMA_CALC, i, j, k);
+    }
+    update_zone(G, i, j, k, Dt, dU, U);
+    msum += U[0];
+    // Newton guess: the predictor's p_f (= ph) holds the unscaled copy of p;
+    // the corrector's p_f is p itself, rescaled in place by the predictor.
+    double pf[HG_NPR];
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) pf[l] = (sub == 0) ? pg[l] : pi[l];
+    double gamma = 0., bsq = 0.;
+    const int ret = utoprim_2d(U, g, G.gam, pf, &gamma, &bsq);
+    const bool ee = G.use_ee && ((pf[UU] < HG_BETA_MIN * bsq) || (pf[RHO] < HG_BETA_MIN * bsq));
+    if (ret != 0 || check_gamma(gamma) == 2 || ee) {
+      // rest of the recover_primitives() tree: queue the zone
+      const int slot = atomicAdd(&G.sc->q_count, 1);
+      if (slot < G.capacity) {
+        G.q_idx[slot] = pack_ijk(i, j, k);
+#pragma unroll
+        for (int l = 0; l < HG_NPR; l++) G.q_U[(long)slot * HG_NPR + l] = U[l];
+      } else {
+        G.sc->err = 2;
+      }
+      continue;
+    }
+    // fast path of recover_primitives (step_ch.c:830-1018, FIXUP_TREE 3)
+    n_full++;
+    G.nfail[NF_USE_FULL_INV * S + o] += 1u;
+    const double rf = G.floors[o], uf = G.floors[S + o];
+    bool fl = false;
+    if (pf[RHO] < rf) { pf[RHO] = rf; fl = true; }
+    if (pf[UU] < uf) { pf[UU] = uf; fl = true; }
+    if (fl) {
+      n_floor++;
+      G.nfail[NF_FLOOR * S + o] += 1u;
+    }
+    int pflag = PF_NONE;
+    if (check_gamma(gamma)) {
+      book(G, NF_GAMMA_MAX, i, j, k);
+      pflag = PF_INTERP_V;
+      flag_zone(G, PF_INTERP_V, i, j, k);
+    }
+    G.p_gamma[o] = gamma;
+    if (pflag == PF_NONE) G.pflag[o] = PF_NONE;
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) p_f[l * S + o] = pf[l];
+  }
+  const double bs = block_sum(msum);
+  if (threadIdx.x == 0) G.blk[blockIdx.x] = bs;
+  const unsigned int c_full = block_count(n_full);
+  const unsigned int c_floor = block_count(n_floor);
+  if (threadIdx.x == 0) {
+    if (c_full) atomicAdd(&G.sc->nfailtot[NF_USE_FULL_INV], (unsigned long long)c_full);
+    if (c_floor) atomicAdd(&G.sc->nfailtot[NF_FLOOR], (unsigned long long)c_floor);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fixup_entropy_eq(), fixup.c:335-454: entropy flux rebuilt from the face
+// states of the six faces (recomputed here; the flux kernel does not store
+// them) and the inversions Utoprim_1d_ee / Utoprim_1d_ee2.
+template <bool RS>
+__device__ __noinline__ double ee_face_flux(const GridDev &G, const double *p_h, int d, int i, int j, int k)
+{
+  double pl[HG_NPR], pr[HG_NPR];
+  face_prims<RS>(G, p_h, d, i, j, k, pl, pr);
+  Geom g;
+  load_geom(G, d, i, j, g);
+  State ql, qr;
+  get_state(pl, g, G.gam, ql);
+  get_state(pr, g, G.gam, qr);
+  const int dim = d + 1;
+  double cmaxl, cminl, cmaxr, cminr;
+  vchar_fast(ql, g, dim, G.gam, &cmaxl, &cminl);
+  vchar_fast(qr, g, dim, G.gam, &cmaxr, &cminr);
+  const double a0 = 0. > cmaxl ? 0. : cmaxl;
+  const double cmax = fabs(a0 > cmaxr ? a0 : cmaxr);
+  const double a1 = 0. > -cminl ? 0. : -cminl;
+  const double cmin = fabs(a1 > -cminr ? a1 : -cminr);
+  const double ctop = cmin > cmax ? cmin : cmax;
+  const double gam = G.gam;
+  double s = (gam - 1.) * pl[UU] * pow(pl[RHO], 1. - gam);
+  const double Ul = s * (g.g * ql.ucon[0]);
+  const double Fl = s * (g.g * ql.ucon[dim]);
+  s = (gam - 1.) * pr[UU] * pow(pr[RHO], 1. - gam);
+  const double Ur = s * (g.g * qr.ucon[0]);
+  const double Fr = s * (g.g * qr.ucon[dim]);
+  if (G.flux == 1) return (cmax * Fl + cmin * Fr - cmax * cmin * (Ur - Ul)) / (cmax + cmin + HG_SMALL);
+  return 0.5 * (Fl + Fr - ctop * (Ur - Ul));
+}
+
+template <bool RS>
+__device__ __noinline__ int fixup_entropy_eq(const GridDev &G, const double *p_h, int i, int j, int k,
+                                             const double *prim_old, double *prim, const Geom &geom,
+                                             const double *Un, double Dt, double *gamma_out)
+{
+  double prim_backup[HG_NPR], gamma;
+  for (int l = 0; l < HG_NPR; l++) prim_backup[l] = prim[l];
+  const double gam = G.gam;
+  gamma_calc(prim_old, geom, &gamma);
+  const double S_old = geom.g * (gam - 1.) * prim_old[UU] * gamma / (geom.alpha * pow(prim_old[RHO], (gam - 1.)));
+  double Fm[3], Fp[3];
+  for (int d = 0; d < 3; d++) Fm[d] = ee_face_flux<RS>(G, p_h, d, i, j, k);
+  for (int d = 0; d < 3; d++) Fp[d] = ee_face_flux<RS>(G, p_h, d, i + (d == 0), j + (d == 1), k + (d == 2));
+  const double Snew = S_old + Dt * (-(Fp[0] - Fm[0]) * G.invdx[1] - (Fp[1] - Fm[1]) * G.invdx[2] -
+                                    (Fp[2] - Fm[2]) * G.invdx[3]);
+  int ret = utoprim_1d_ee(Un, Snew, geom, gam, prim, &gamma);
+  if ((!ret) && (check_gamma(gamma) == 2)) {
+    for (int l = 0; l < HG_NPR; l++) prim[l] = prim_backup[l];
+    ret = 1;
+    gamma = 1.;
+  }
+  if (ret) {
+    ret = utoprim_1d_ee2(Un, Snew, geom, gam, prim, &gamma);
+    if ((!ret) && (check_gamma(gamma) == 2)) {
+      for (int l = 0; l < HG_NPR; l++) prim[l] = prim_backup[l];
+      ret = 1;
+    }
+    if (ret) gamma = 1.;
+  }
+  *gamma_out = gamma;
+  if (!ret) book(G, NF_USE_EE, i, j, k);
+  return ret;
+}
+
+// recover_primitives(), step_ch.c:801-1024 (FIXUP_TREE 3), full tree.
+template <bool RS>
+__global__ void __launch_bounds__(HG_BLK) k_fallback(GridDev G, int sub, double dtfac, const double *__restrict__ p_h,
+                                                     double *__restrict__ p_f)
+{
+  const int n = min(G.sc->q_count, (int)G.capacity);
+  const double Dt = dtfac * G.sc->dt;
+  const long S = G.S;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    int i, j, k;
+    unpack_ijk(G.q_idx[e], i, j, k);
+    const long o = off3(G, i, j, k);
+    double U[HG_NPR], pf[HG_NPR], pg[HG_NPR], pold[HG_NPR], pf2[HG_NPR];
+    for (int l = 0; l < HG_NPR; l++) {
+      U[l] = G.q_U[(long)e * HG_NPR + l];
+      pold[l] = G.p[l * S + o];
+      pf[l] = (sub == 0 || !RS) ? pold[l] : rs_roundtrip(G, pold[l], l, i);
+      pg[l] = pf[l];
+    }
+    Geom g;
+    load_geom(G, 3, i, j, g);
+    double gamma = 0., bsq = 0.;
+    int ret = utoprim_2d(U, g, G.gam, pf, &gamma, &bsq);
+    if ((!ret) && (check_gamma(gamma) == 2)) {
+      for (int l = 0; l < B1; l++) pf[l] = pg[l];
+      ret = 1;
+      gamma = 1.;
+    }
+    if (ret) {
+      ret = utoprim_1d(U, g, G.gam, pf, &gamma, &bsq);
+      if ((!ret) && (check_gamma(gamma) == 2)) {
+        for (int l = 0; l < B1; l++) pf[l] = pg[l];
+        ret = 1;
+      }
+      if (ret) gamma = 1.;
+    }
+    double pgam = gamma;
+    int use_ee = 0;
+    if (G.use_ee && (ret || (pf[UU] < HG_BETA_MIN * bsq) || (pf[RHO] < HG_BETA_MIN * bsq))) use_ee = 1;
+    int pflag = PF_NONE;
+    bool done = false;
+    if (!use_ee) {
+      if (!ret) book(G, NF_USE_FULL_INV, i, j, k);
+      else {
+        book(G, NF_UTOPRIM, i, j, k);
+        pflag = PF_INTERP_PRIM;
+      }
+    } else {
+      if (!ret) {
+        for (int l = 0; l < HG_NPR; l++) pf2[l] = pf[l];
+      } else {
+        book(G, NF_UTOPRIM, i, j, k);
+      }
+      for (int l = 0; l < B1; l++) pf[l] = pg[l];
+      const int ret_ee = fixup_entropy_eq<RS>(G, p_h, i, j, k, pold, pf, g, U, Dt, &gamma);
+      if (ret_ee) {
+        if (ret) {
+          book(G, NF_UTOPRIM_EE, i, j, k);
+          pflag = PF_INTERP_PRIM;
+          done = true;
+        } else {
+          book(G, NF_UTOPRIM_EE, i, j, k);
+          for (int l = 0; l < HG_NPR; l++) pf[l] = pf2[l];
+          gamma = pgam;
+          book(G, NF_USE_FULL_INV, i, j, k);
+        }
+      }
+    }
+    if (!done) {
+      pgam = gamma;
+      const double rf = G.floors[o], uf = G.floors[S + o];
+      bool fl = false;
+      if (pf[RHO] < rf) { pf[RHO] = rf; fl = true; }
+      if (pf[UU] < uf) { pf[UU] = uf; fl = true; }
+      if (fl) book(G, NF_FLOOR, i, j, k);
+      if (check_gamma(gamma)) {
+        book(G, NF_GAMMA_MAX, i, j, k);
+        pflag = PF_INTERP_V;
+      }
+    }
+    G.p_gamma[o] = pgam;
+    if (pflag != PF_NONE) flag_zone(G, pflag, i, j, k);
+    else G.pflag[o] = PF_NONE;
+    for (int l = 0; l < HG_NPR; l++) p_f[l * S + o] = pf[l];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Boundary conditions, bounds.c:58-211: every ghost zone copies the zone
+// reached by applying the per-direction map (outflow: clamp to the physical
+// range; periodic: wrap) in each direction.  The reference fills x1, then x2
+// over all i, then x3 over all i,j, which composes to the same map.
+__device__ __forceinline__ int bc_map(int x, int n, int periodic)
+{
+  const int s = HG_NGH, e = n + HG_NGH - 1;
+  if (x < s) return periodic ? x + n : s;
+  if (x > e) return periodic ? x - n : e;
+  return x;
+}
+
+__global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict__ pa, int conditional)
+{
+  if (conditional && !G.sc->bnd_phys) return;
+  const int T0 = G.T[0], T1 = G.T[1], T2 = G.T[2];
+  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
+  const long c1 = (long)T0 * T1 * (T2 - (G.deg[2] ? 1 : N2));
+  const long c2 = (long)T0 * (T1 - (G.deg[1] ? 1 : N1)) * (G.deg[2] ? 1 : N2);
+  const long c3 = (long)(T0 - (G.deg[0] ? 1 : N0)) * (G.deg[1] ? 1 : N1) * (G.deg[2] ? 1 : N2);
+  const long total = c1 + c2 + c3;
+  const int per = (G.bc == 1);
+  const int fl = G.sc->failure_exists;
+  const long S = G.S;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    int i, j, k;  // stored indices
+    if (t < c1) {
+      i = (int)(t % T0);
+      j = (int)((t / T0) % T1);
+      const int kg = (int)(t / ((long)T0 * T1));
+      k = kg < HG_NGH ? kg : kg + N2;
+    } else if (t < c1 + c2) {
+      const long u = t - c1;
+      i = (int)(u % T0);
+      const int jg = (int)((u / T0) % (T1 - N1));
+      j = jg < HG_NGH ? jg : jg + N1;
+      k = HG_NGH + (int)(u / ((long)T0 * (T1 - N1)));
+    } else {
+      const long u = t - c1 - c2;
+      const int ig = (int)(u % (T0 - N0));
+      i = ig < HG_NGH ? ig : ig + N0;
+      j = HG_NGH + (int)((u / (T0 - N0)) % N1);
+      k = HG_NGH + (int)(u / ((long)(T0 - N0) * N1));
+    }
+    // degenerate directions have no ghosts, so these are reference indices
+    const int si = G.deg[0] ? i : bc_map(i, N0, per);
+    const int sj = G.deg[1] ? j : bc_map(j, N1, per);
+    const int sk = G.deg[2] ? k : bc_map(k, N2, per);
+    const long od = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+    const long os = (long)si * G.st[0] + (long)sj * G.st[1] + (long)sk * G.st[2];
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) pa[l * S + od] = pa[l * S + os];
+    // pflag ghosts are copies while a failure exists in this substep; otherwise
+    // every pflag of the reference is zero (step_ch.c:65-69, 123-127)
+    G.pflag[od] = fl ? G.pflag[os] : 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fixup_interp_v / fixup_interp_prim (fixup.c:499-761) over the flagged list.
+// A zone only reads unflagged neighbours, which no thread writes, so the
+// zones are independent and the order of the reference's loop is immaterial.
+__global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict__ pv)
+{
+  const int n = min(G.sc->fl_count, (int)G.capacity);
+  const long S = G.S;
+  const int ngood_min_tab[4] = {13, 9, 6, 4};
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    int i, j, k;
+    unpack_ijk(G.fl_idx[e], i, j, k);
+    const long o = off3(G, i, j, k);
+    const int which = G.pflag[o];
+    if (which != PF_INTERP_V && which != PF_INTERP_PRIM) continue;
+    const int lo = which == PF_INTERP_PRIM ? 0 : U1, hi = which == PF_INTERP_PRIM ? B1 - 1 : U3;
+    unsigned int good = 0;  // bit (13 + ii + 3*(jj + 3*kk)) set if that neighbour is usable
+    for (int kk = -1; kk <= 1; kk++)
+      for (int jj = -1; jj <= 1; jj++)
+        for (int ii = -1; ii <= 1; ii++)
+          if (!G.pflag[off3(G, i + ii, j + jj, k + kk)]) good |= 1u << (13 + ii + 3 * (jj + 3 * kk));
+    int ngood = 0;
+    for (int m = 1; m <= 13; m++) {
+      if (((good >> (13 + m)) & 1u) && ((good >> (13 - m)) & 1u)) ngood++;
+      else good &= ~((1u << (13 + m)) | (1u << (13 - m)));
+    }
+    // icurr/jcurr/kcurr of the reference: the zone, or the last usable
+    // neighbour visited by the gamma loop once that loop has run.
+    int ci = i, cj = j, ck = k;
+    double pc[HG_NPR], pold[HG_NPR];
+    for (int l = 0; l < HG_NPR; l++) pc[l] = pv[l * S + o];
+    for (int l = lo; l <= hi; l++) pold[l] = pc[l];
+    Geom g;
+    load_geom(G, 3, i, j, g);
+    double gamma, f, gamma_old;
+    int i_ret;
+    const int ngood_min = ngood_min_tab[G.nsd];
+    if (which == PF_INTERP_PRIM && ngood < ngood_min) {
+      gamma_calc(pc, g, &gamma);
+      G.p_gamma[o] = gamma;
+      book(G, NF_INTERP_PRIM, ci, cj, ck);
+      continue;
+    }
+    if (which == PF_INTERP_V && ngood < ngood_min) {
+      double pg = G.p_gamma[o];
+      f = sqrt((HG_GAMMAMAX - 1.) * (HG_GAMMAMAX + 1.) / ((pg - 1.) * (pg + 1.)));
+      pc[U1] *= f;
+      pc[U2] *= f;
+      pc[U3] *= f;
+      G.p_gamma[o] = HG_GAMMAMAX;
+      book(G, NF_GAMMA_MAX, ci, cj, ck);
+      book(G, NF_INTERP_V, ci, cj, ck);
+      for (int l = U1; l <= U3; l++) pv[l * S + o] = pc[l];
+      continue;
+    }
+    for (int l = lo; l <= hi; l++) pc[l] = 0.;
+    // the reference sums over ii (outer), jj, kk (inner)
+    for (int ii = -1; ii <= 1; ii++)
+      for (int jj = -1; jj <= 1; jj++)
+        for (int kk = -1; kk <= 1; kk++)
+          if ((good >> (13 + ii + 3 * (jj + 3 * kk))) & 1u) {
+            const long on = off3(G, i + ii, j + jj, k + kk);
+            for (int l = lo; l <= hi; l++) pc[l] += pv[l * S + on];
+          }
+    const int ng2 = ngood * 2;
+    for (int l = lo; l <= hi; l++) pc[l] /= ng2;
+    i_ret = gamma_calc(pc, g, &gamma);
+    if (check_gamma(gamma)) {
+      gamma_old = gamma;
+      gamma = 0.;
+      int ngood2 = 0;
+      for (int ii = -1; ii <= 1; ii++)
+        for (int jj = -1; jj <= 1; jj++)
+          for (int kk = -1; kk <= 1; kk++)
+            if ((good >> (13 + ii + 3 * (jj + 3 * kk))) & 1u) {
+              Geom g2;
+              load_geom(G, 3, i + ii, j + jj, g2);
+              ci = i + ii;
+              cj = j + jj;
+              ck = k + kk;
+              const long on = off3(G, i + ii, j + jj, k + kk);
+              double pn[HG_NPR];
+              for (int l = 0; l < HG_NPR; l++) pn[l] = pv[l * S + on];
+              i_ret = gamma_calc(pn, g2, &f);
+              if (!i_ret) {
+                gamma += f;
+                ngood2++;
+              }
+            }
+      gamma /= ngood2;
+      f = sqrt((gamma - 1.) * (gamma + 1.) / ((gamma_old - 1.) * (gamma_old + 1.)));
+      pc[U1] *= f;
+      pc[U2] *= f;
+      pc[U3] *= f;
+      i_ret = gamma_calc(pc, g, &gamma);
+    }
+    if (which == PF_INTERP_PRIM) {
+      if (i_ret) {
+        for (int l = U1; l <= U3; l++) pc[l] = pold[l];
+        gamma_calc(pc, g, &gamma);
+        book(G, NF_INTERP_PRIM, ci, cj, ck);
+      }
+      book(G, NF_USE_INTERP_PRIM, ci, cj, ck);
+      if ((!i_ret) && check_gamma(gamma)) {
+        f = sqrt((HG_GAMMAMAX - 1.) * (HG_GAMMAMAX + 1.) / ((gamma - 1.) * (gamma + 1.)));
+        pc[U1] *= f;
+        pc[U2] *= f;
+        pc[U3] *= f;
+        gamma = HG_GAMMAMAX;
+        book(G, NF_GAMMA_MAX, ci, cj, ck);
+      }
+      G.p_gamma[o] = gamma;
+    } else {
+      if (i_ret || check_gamma(gamma)) {
+        for (int l = U1; l <= U3; l++) pc[l] = pold[l];
+        const double pg = G.p_gamma[o];
+        f = sqrt((HG_GAMMAMAX - 1.) * (HG_GAMMAMAX + 1.) / ((pg - 1.) * (pg + 1.)));
+        pc[U1] *= f;
+        pc[U2] *= f;
+        pc[U3] *= f;
+        G.p_gamma[o] = HG_GAMMAMAX;
+        book(G, NF_GAMMA_MAX, ci, cj, ck);
+        book(G, NF_INTERP_V, ci, cj, ck);
+      } else {
+        book(G, NF_USE_INTERP_V, ci, cj, ck);
+        G.p_gamma[o] = gamma;
+      }
+    }
+    for (int l = lo; l <= hi; l++) pv[l * S + o] = pc[l];
+  }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_begin(DevScalars *sc)
+{
+  sc->maxs[0] = sc->maxs[1] = sc->maxs[2] = sc->maxs[3] = 0ull;
+  sc->failure_exists = 0;
+  sc->ftype[0] = sc->ftype[1] = sc->ftype[2] = 0;
+  sc->bnd_phys = 0;
+  sc->q_count = 0;
+  sc->fl_count = 0;
+}
+
+// t += dx[0]; dx[0] = timestep() (step_ch.c:218-223, 546-623); M_tot.
+__global__ void k_timestep(GridDev G, int nblk)
+{
+  __shared__ double red[256];
+  double s = 0.;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += G.blk[b];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    DevScalars *sc = G.sc;
+    sc->m_tot = red[0];
+    const double c1 = __longlong_as_double((long long)sc->maxs[1]);
+    const double c2 = __longlong_as_double((long long)sc->maxs[2]);
+    const double c3 = __longlong_as_double((long long)sc->maxs[3]);
+    sc->last_maxs[1] = c1;
+    sc->last_maxs[2] = c2;
+    sc->last_maxs[3] = c3;
+    const double dt_old = sc->dt;
+    const double t = sc->t + dt_old;
+    const double dtsqij =
+        sqrt((1. / 3.) / ((c1 * c1) / (G.dx[1] * G.dx[1]) + (c2 * c2) / (G.dx[2] * G.dx[2]) + (c3 * c3) / (G.dx[3] * G.dx[3])));
+    double dtt = G.cour * dtsqij;
+    if (dtt > HG_SAFE * dt_old) dtt = HG_SAFE * dt_old;
+    if (t + dtt > (G.grid_length[0] + G.startx[0])) dtt = G.grid_length[0] + G.startx[0] - t;
+    sc->t = t;
+    sc->dt = dtt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launch sequence of one step.
+static inline void mark(EventRec *r, int cls, cudaStream_t s)
+{
+  if (!r || r->n >= r->cap) return;
+  r->cls[r->n] = cls;
+  cudaEventRecord((cudaEvent_t)r->ev[r->n], s);
+  r->n++;
+}
+
+static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int sub, EventRec *R)
+{
+  const double *ph = sub == 0 ? G.p : G.ph;
+  double *pf = sub == 0 ? G.ph : G.p;
+  const double dtfac = sub == 0 ? 0.5 : 1.0;
+  mark(R, KC_MISC, s);
+  k_begin<<<1, 1, 0, s>>>(G.sc);
+  for (int d = 0; d < 3; d++) {
+    int lo[3], n[3];
+    unsigned int mult = 1;
+    for (int a = 0; a < 3; a++) {
+      if (G.deg[a]) {
+        lo[a] = HG_NGH;
+        n[a] = 1;
+        mult *= (a == d) ? 2u : (G.ct_para ? 1u + 2u * HG_NGH : 3u);
+      } else if (a == d) {
+        lo[a] = HG_NGH;
+        n[a] = G.N[a] + 1;
+      } else if (G.ct_para) {
+        lo[a] = 0;
+        n[a] = G.N[a] + 2 * HG_NGH;
+      } else {
+        lo[a] = HG_NGH - 1;
+        n[a] = G.N[a] + 2;
+      }
+    }
+    mark(R, KC_FLUX, s);
+    if (G.rescale)
+      k_flux<true><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, d, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult);
+    else
+      k_flux<false><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, d, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult);
+  }
+  {
+    int lo[3], n[3];
+    for (int a = 0; a < 3; a++) {
+      lo[a] = HG_NGH;
+      n[a] = G.deg[a] ? 1 : G.N[a] + 1;
+    }
+    mark(R, KC_EMF, s);
+    k_emf<<<L.grid_emf, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2]);
+  }
+  mark(R, KC_UPDATE, s);
+  if (G.rescale) k_update<true><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  else k_update<false><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  mark(R, KC_FALLBACK, s);
+  if (G.rescale) k_fallback<true><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  else k_fallback<false><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  mark(R, KC_BOUNDS, s);
+  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, pf, 0);
+  mark(R, KC_FIXUP, s);
+  k_fixup<<<L.grid_fix, HG_BLK, 0, s>>>(G, pf);
+  mark(R, KC_BOUNDS, s);
+  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, pf, 1);
+}
+
+void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R)
+{
+  launch_substep(G, L, s, 0, R);
+  launch_substep(G, L, s, 1, R);
+  mark(R, KC_MISC, s);
+  k_timestep<<<1, 256, 0, s>>>(G, L.grid_upd);
+  mark(R, KC_END, s);
+}
+
+}  // namespace hg

@@ -1,0 +1,147 @@
+/* harmgpu.h -- C ABI of libharmgpu, the B200 (sm_100a) step engine that
+ * replaces HARM3D's step_ch()/advance() path.
+ *
+ * Caller side of the reference (scnastro/coolharm3d, paths relative to src/):
+ *   - main.c:81 calls `void step_ch(void)` (step_ch.c:50-234) once per step;
+ *     everything flows through globals (p, dx[0], t, pflag, nfail, nfailtot,
+ *     p_gamma, M_tot).  A driver built with USE_GPU_STEP calls hg_step()
+ *     instead and keeps the primitive variables resident on the GPU between
+ *     steps; it downloads them only before diag()/restart_write() write them.
+ *   - Geometry (geom_arr, conn: metric.c:4111-4265) and coordinate floors
+ *     (coord_arr[].rhoflr/uuflr: coord.c:3792-3796) are computed by the
+ *     driver's own init and handed over once with hg_set_geometry() and
+ *     hg_set_cell_data(); hg_build_* compute the same tables without the
+ *     driver.
+ *
+ * Conventions: every entry point returns 0 (HG_OK) or a negative HG_ERR_*
+ * code; hg_strerror() names it.  A caller maps a negative return to its own
+ * fail(FAIL_BASIC,0) (diag.c:458-470).  One handle per grid; a handle is used
+ * by one host thread at a time.  Arrays in the reference's layout are
+ * N1TOT x N2TOT x N3TOT cells (NG = 3 ghost cells on each side in every
+ * direction, N*TOT = N* + 6) with index ((i*N2TOT + j)*N3TOT + k), and, for
+ * primitives, the 8 variables innermost: exactly a flattened p[i][j][k][l].
+ */
+#ifndef HARMGPU_H
+#define HARMGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HG_OK 0
+#define HG_ERR_CUDA (-1)        /* a CUDA runtime call failed */
+#define HG_ERR_BADARG (-2)      /* invalid argument or unsupported switch value */
+#define HG_ERR_TIMEOUT (-3)     /* a bounded device-side wait expired */
+#define HG_ERR_NOMEM (-4)       /* device memory could not be allocated */
+#define HG_ERR_STATE (-5)       /* call out of order (e.g. step before geometry) */
+#define HG_ERR_DEVICE (-6)      /* a kernel reported an internal error status */
+
+#define HG_NP 8                 /* NP, macros.h:38 */
+#define HG_NG 3                 /* NG, macros.h:39 */
+#define HG_NFAIL 15             /* N_NFAIL, macros.h:258 */
+#define HG_NGEOM 42             /* doubles per struct of_geom (globals.h:90-98) */
+
+#define HG_PREC_FP64 0          /* every operation in IEEE double, no FMA: bit-identical to the reference */
+#define HG_PREC_MIXED 1         /* reconstruction + HLL flux in FP32, everything else FP64 */
+
+/* Run description: the options.h switches of the path plus init_base() values. */
+typedef struct hg_grid_desc {
+  int32_t n1, n2, n3;           /* physical zones: N1, N2, N3 (harm_mpi.c:1445 myargs) */
+  int32_t recon_type;           /* RECON_TYPE_CHOICE 0..5 (options.h:148-155) */
+  int32_t flux_type;            /* FLUX_TYPE_CHOICE: 0 LF, 1 HLLE (options.h:168-172) */
+  int32_t use_flux_ct_para;     /* USE_FLUX_CT_PARA (options.h:165) */
+  int32_t bc_type;              /* BC_TYPE_CHOICE: 0 CARTESIAN_OUTFLOW, 1 CARTESIAN_PERIODIC,
+                                   10 SPHERICAL_OUTFLOW3 (options.h:98-124) */
+  int32_t metric_dim;           /* METRIC_DIM: 0 (one geometry for every cell) or 2
+                                   (axisymmetric tables over i,j) (macros.h:47-53) */
+  int32_t use_entropy_eq;       /* USE_ENTROPY_EQ (options.h:209) */
+  int32_t cooling;              /* USE_COOLING_FUNCTION: 0 or 1 (options.h:192) */
+  int32_t rescale_r;            /* RESCALE_R (options.h:267) */
+  int32_t precision;            /* HG_PREC_FP64 or HG_PREC_MIXED */
+  double gam;                   /* adiabatic index */
+  double cour;                  /* Courant number */
+  double dx[4];                 /* dx[0] = first time step, dx[1..3] = zone sizes */
+  double startx[4];             /* numerical (ghost-inclusive) left edge */
+  double grid_length[4];        /* GridLength[0] = final time */
+  double t;                     /* initial time */
+  int32_t device;               /* CUDA device ordinal */
+  int32_t reserved;
+} hg_grid_desc;
+
+typedef struct hg_handle hg_handle;
+
+/* Validate the description, select the device and allocate the resident grid.
+ * Replaces alloc_grid_arrays() (decomp.c:140-404) for the step's arrays. */
+int hg_init(const hg_grid_desc *desc, hg_handle **out);
+
+/* Static geometry: n_geom structs of HG_NGEOM doubles in struct of_geom
+ * order (gcon[16], gcov[16], g, g_inv, alpha, beta[3], ncon[4]) and
+ * GEOM_ID order (macros.h:592-601): 1 struct for metric_dim 0,
+ * 5*N1TOT*N2TOT for metric_dim 2.  conn: n_conn x 64 doubles in CONN_ID
+ * order (macros.h:575-586; n_conn = N1*N2 for metric_dim 2, else ignored).
+ * Replaces the per-cell reads of geom_arr/conn done by get_geometry(). */
+int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom, const double *conn, int64_t n_conn);
+
+/* Per-cell centre data in the reference layout, 6 doubles per cell:
+ * rhoflr, uuflr, r, x1, x2, x3 (struct of_coord, coord.c:3754-3800);
+ * rface[N1TOT]: x[RR] at FACE1 (RESCALE_R only, else NULL). */
+int hg_set_cell_data(hg_handle *h, const double *cell6, const double *rface);
+
+/* Primitive variables in the reference layout (flattened p[i][j][k][l]).
+ * Upload is hg_upload_prims; download is what diag()/restart_write() need. */
+int hg_upload_prims(hg_handle *h, const double *p);
+int hg_download_prims(hg_handle *h, double *p);
+/* Same through the reference's own pointer tree double ****p (decomp.c:148). */
+int hg_upload_prims_tree(hg_handle *h, double ****p);
+int hg_download_prims_tree(hg_handle *h, double ****p);
+
+/* Set the time and next time step (t, dx[0]); e.g. after restart_init(). */
+int hg_set_time(hg_handle *h, double t, double dt);
+
+/* Advance nsteps full RK2 steps: the whole of step_ch() (predictor,
+ * boundaries, fixups, corrector, boundaries, fixups, timestep()) on the
+ * device.  On return *t and *dt (either may be NULL) hold t and dx[0]. */
+int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt);
+
+/* Failure bookkeeping of fail() (diag.c:159-500): nfailtot[N_NFAIL]
+ * accumulated since the last upload, pflag (int32 per cell), p_gamma
+ * (double per cell), nfail (int32, [N_NFAIL][cells]). */
+int hg_get_fail_counts(hg_handle *h, uint64_t nfailtot[HG_NFAIL]);
+int hg_download_pflag(hg_handle *h, int32_t *pflag);
+int hg_download_gamma(hg_handle *h, double *p_gamma);
+int hg_download_nfail(hg_handle *h, int32_t *nfail);
+
+/* Diagnostics of the last step: M_tot (sum of U[RHO] over the domain after
+ * the corrector, step_ch.c:402) and the per-direction maximum
+ * characteristic speeds that set dx[0] (step_ch.c:716-724). */
+int hg_get_diag(hg_handle *h, double *m_tot, double max_char_speed[3]);
+
+/* Device time of the last hg_step call in milliseconds (CUDA events). */
+int hg_last_step_ms(hg_handle *h, double *ms);
+
+/* Per-kernel timing.  hg_profile(h, 1) makes every following hg_step record a
+ * CUDA event on the engine's stream before each kernel; hg_kernel_times()
+ * returns, per kernel class (flux, emf, update, fallback, bounds, fixup,
+ * misc), the summed milliseconds and the number of launches since the last
+ * hg_profile() call.  The reference has no counterpart (it times with
+ * gettimeofday around whole routines, macros.h:620-657). */
+#define HG_NKCLASS 7
+int hg_profile(hg_handle *h, int32_t enable);
+int hg_kernel_times(hg_handle *h, double ms[HG_NKCLASS], int64_t launches[HG_NKCLASS]);
+
+void hg_destroy(hg_handle *h);
+const char *hg_strerror(int code);
+
+/* Host-side geometry builders (the init-time work of calc_all_geom(),
+ * metric.c:4111-4265, for the metrics the engine supports).
+ * Minkowski Cartesian with COORD_IDENTITY: geom = 1 struct (HG_NGEOM),
+ * cell6 = N1TOT*N2TOT*N3TOT*6 with the r-dependent floors RHOMIN r^-1.5,
+ * UUMIN r^-2.5 (options.h:233-240). */
+int hg_build_geometry_minkowski(const hg_grid_desc *desc, double *geom, double *cell6);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HARMGPU_H */

@@ -1,0 +1,29 @@
+"""Loading of the golden fixtures of tests/golden (made by make_golden.py)."""
+import glob
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    d = {k: z[k] for k in z.files}
+    d["config"] = str(d["config"])
+    d["n"] = tuple(int(x) for x in d["n"])
+    d["steps"] = int(d["steps"])
+    d["sw"] = {k[3:]: int(d[k]) for k in z.files if k.startswith("sw_")}
+    for k in ("t0", "dt0", "t", "dt", "m_tot", "gam", "cour"):
+        d[k] = float(d[k])
+    return d
+
+
+def geomd(f, cell6=None):
+    """Descriptor dict for harmtest.Oracle from a fixture."""
+    return dict(gam=f["gam"], cour=f["cour"], grid_length=f["grid_length"], startx=f["startx"], dx=f["dx"],
+                geom=f["geom"], conn=f["conn"], cell6=cell6)

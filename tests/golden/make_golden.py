@@ -1,0 +1,84 @@
+#!/usr/bin/env python3
+"""Generate tests/golden/*.npz from the reference's own CPU build.
+
+Run where the reference sources are available (python oracle/build_ref.py
+first).  Each fixture holds the state handed to the reference's step_ch()
+(after its own init.*.c, or a seeded "stress" state loaded through
+oracle/ref_probe.c), the state after `steps` steps (all cells, ghosts
+included), pflag, p_gamma, nfail, nfailtot, t, dx[0], M_tot, the run
+parameters and the reference's geometry/floor tables.
+
+Stress states draw rho, u from log-uniform ranges down to 1e-6/1e-7,
+velocities with 4-vector magnitudes up to ~30 and fields up to ~3, so that
+the inversion fallbacks, entropy fix, floors, gamma ceiling and both
+interpolation fixups all fire.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+import harmtest as ht  # noqa: E402
+
+CASES = [
+    # name, config, grid, steps, stress seed (None = reference init)
+    ("balsara1_n128_s1", "balsara1", (128, 1, 1), 1, None),
+    ("balsara1_n128_s60", "balsara1", (128, 1, 1), 60, None),
+    ("balsara1_lf_n64_s20", "balsara1_lf", (64, 1, 1), 20, None),
+    ("balsara1_stress_n64_s2", "balsara1", (64, 1, 1), 2, 11),
+    ("linwave_12x10x8_s2", "linwave", (12, 10, 8), 2, None),
+    ("linwave_stress_10x8x6_s2", "linwave", (10, 8, 6), 2, 7),
+    ("linwave_vl_stress_8x8x8_s2", "linwave_vl", (8, 8, 8), 2, 5),
+    ("linwave_2d_16x16x1_s3", "linwave", (16, 16, 1), 3, None),
+]
+
+
+def stress_state(p, seed):
+    rng = np.random.default_rng(seed)
+    p = p.copy()
+    sh = p.shape[:3]
+    p[..., 0] = 10 ** rng.uniform(-6, 0, sh)
+    p[..., 1] = 10 ** rng.uniform(-7, 0, sh)
+    p[..., 2:5] = rng.normal(0, 1.0, sh + (3,)) * 10 ** rng.uniform(-2, 1.5, sh + (1,))
+    p[..., 5:8] = rng.normal(0, 1, sh + (3,)) * 10 ** rng.uniform(-2, 0.5, sh + (1,))
+    # a direction with one zone holds ghost copies of that zone in the reference
+    for a in range(3):
+        if sh[a] == 1 + 2 * ht.NG:
+            idx = [slice(None)] * 3
+            idx[a] = slice(ht.NG, ht.NG + 1)
+            p[...] = np.broadcast_to(p[tuple(idx)], p.shape)
+    return p
+
+
+def make(name, cfg, n, steps, seed):
+    r0 = ht.run_ref(cfg, n, 1, dumps=[0], want_geom=True)
+    s0 = r0["states"][0]
+    geom = r0["geom"]
+    if seed is None:
+        load = None
+        p0, t0, dt0 = s0["p"], s0["t"], s0["dt"]
+    else:
+        p0 = stress_state(s0["p"], seed)
+        t0, dt0 = s0["t"], 1e-4
+        load = dict(p=p0, t=t0, dt=dt0)
+    r = ht.run_ref(cfg, n, steps, load=load)
+    s = r["states"][steps]
+    sw = ht.CONFIG_SWITCHES[cfg]
+    out = dict(
+        config=cfg, n=np.array(n), steps=steps, p0=p0, t0=t0, dt0=dt0,
+        p=s["p"], pflag=s["pflag"], gamma=s["gamma"], nfail=s["nfail"], nfailtot=s["nfailtot"],
+        t=s["t"], dt=s["dt"], m_tot=s["m_tot"],
+        gam=geom["gam"], cour=geom["cour"], grid_length=geom["grid_length"], startx=geom["startx"],
+        dx=geom["dx"], geom=geom["geom"], conn=geom["conn"],
+        **{"sw_" + k: v for k, v in sw.items()})
+    # floors at every cell centre (the engine's builder is checked against these)
+    out["cell_floors"] = geom["cell6"][..., :2]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "nfailtot", s["nfailtot"].tolist())
+
+
+if __name__ == "__main__":
+    for c in CASES:
+        make(*c)

@@ -1,0 +1,124 @@
+"""GPU parity: the sm_100a engine (through the C ABI) against the reference's
+golden fixtures and against the C oracle on the same seeded inputs.
+
+FP64 form: bit-identical primitives (every cell, ghosts included), pflag,
+p_gamma, nfail, nfailtot, t and dx[0].  M_tot is a reduction whose
+summation order differs (per-block partials): relative tolerance 1e-13.
+"""
+import numpy as np
+import pytest
+
+import coolharm3d_b200 as hg
+import fixtures
+import harmtest as ht
+
+pytestmark = pytest.mark.gpu
+
+SW_TO_DESC = dict(recon="recon", flux="flux", ct_para="ct_para", bc="bc", metric_dim="metric_dim", ee="use_ee")
+
+
+def engine_for(n, sw, prm, p0, t0, dt0):
+    d = hg.make_desc(n, prm["gam"], prm["cour"], prm["dx"], prm["startx"], prm["grid_length"], t=t0,
+                     recon=sw["recon"], flux=sw["flux"], ct_para=sw["ct_para"], bc=sw["bc"],
+                     metric_dim=sw["metric_dim"], use_ee=sw["ee"])
+    geom, cell6 = hg.minkowski_tables(d)
+    e = hg.Engine(d)
+    e.set_geometry(geom)
+    e.set_cell_data(cell6)
+    e.upload(p0)
+    e.set_time(t0, dt0)
+    return e, cell6
+
+
+def assert_same(e, ref, n, check_nfail=True):
+    p = e.download()
+    bad = np.argwhere(p != ref["p"])
+    assert bad.size == 0, "first mismatches %s" % bad[:5].tolist()
+    assert np.array_equal(e.pflag(), ref["pflag"])
+    assert np.array_equal(ht.interior(e.gamma(), n), ht.interior(ref["gamma"], n))
+    assert e.fail_counts().tolist() == ref["nfailtot"].tolist()
+    if check_nfail:
+        if min(n) > 1:
+            assert np.array_equal(e.nfail(), ref["nfail"])
+        else:
+            nf = e.nfail()
+            for s in range(hg.NFAIL):
+                assert np.array_equal(ht.interior(nf[s], n), ht.interior(ref["nfail"][s], n)), s
+
+
+@pytest.mark.parametrize("name", fixtures.names())
+def test_engine_matches_reference_fixture(name):
+    f = fixtures.load(name)
+    e, _ = engine_for(f["n"], f["sw"], f, f["p0"], f["t0"], f["dt0"])
+    t, dt = e.step(f["steps"])
+    assert t == f["t"] and dt == f["dt"]
+    assert_same(e, f, f["n"])
+    m, _ = e.diag()
+    assert abs(m - f["m_tot"]) <= 1e-13 * abs(f["m_tot"])
+
+
+def _oracle_case(cfg, n, steps, seed, split=False):
+    f0 = fixtures.load({"balsara1": "balsara1_n128_s1", "balsara1_lf": "balsara1_lf_n64_s20",
+                        "linwave": "linwave_12x10x8_s2", "linwave_vl": "linwave_vl_stress_8x8x8_s2"}[cfg])
+    sw = f0["sw"]
+    # run parameters of the configuration at this grid size (init_base of the setup)
+    L = f0["grid_length"]
+    dx = [1e-5] + [L[a] / n[a - 1] for a in (1, 2, 3)]
+    start0 = f0["startx"] + 3 * np.array(f0["dx"])  # physical left edge
+    startx = [0.0] + [start0[a] - 3 * dx[a] for a in (1, 2, 3)]
+    prm = dict(gam=f0["gam"], cour=f0["cour"], dx=dx, startx=startx, grid_length=L)
+    shape = tuple(x + 6 for x in n)
+    rng = np.random.default_rng(seed)
+    p0 = np.empty(shape + (8,))
+    x = startx[1] + (np.arange(shape[0]) + 0.5) * dx[1]
+    y = startx[2] + (np.arange(shape[1]) + 0.5) * dx[2]
+    z = startx[3] + (np.arange(shape[2]) + 0.5) * dx[3]
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    ph = np.cos(2 * np.pi * (X + Y + Z))
+    p0[..., 0] = 1 + 0.3 * ph
+    p0[..., 1] = 1 + 0.2 * np.sin(2 * np.pi * X)
+    p0[..., 2] = 0.2 * ph
+    p0[..., 3] = 0.1 * np.sin(2 * np.pi * Y)
+    p0[..., 4] = -0.1 * ph
+    p0[..., 5] = 0.6
+    p0[..., 6] = 0.3 * np.cos(2 * np.pi * Z)
+    p0[..., 7] = 0.2 * np.sin(2 * np.pi * X)
+    if seed:  # sprinkle extreme zones
+        m = rng.random(shape) < 0.05
+        p0[m, 0] = 10 ** rng.uniform(-7, -2, m.sum())
+        p0[m, 2:5] = rng.normal(0, 15, (m.sum(), 3))
+    for a in range(3):
+        if n[a] == 1:
+            idx = [slice(None)] * 3
+            idx[a] = slice(3, 4)
+            p0[...] = np.broadcast_to(p0[tuple(idx)], p0.shape)
+    e, cell6 = engine_for(n, sw, prm, p0, 0.0, 1e-4)
+    o = ht.Oracle(n, sw, dict(prm, geom=f0["geom"], conn=f0["conn"], cell6=cell6))
+    o.set_state(p0, 0.0, 1e-4)
+    if split:
+        for _ in range(steps):
+            e.step(1)
+    else:
+        e.step(steps)
+    o.step(steps)
+    return e, o.state()
+
+
+@pytest.mark.parametrize("cfg,n,steps,seed", [
+    ("linwave", (40, 36, 28), 3, 0),
+    ("linwave", (24, 20, 16), 2, 5),
+    ("linwave_vl", (20, 18, 12), 2, 9),
+    ("balsara1", (1024, 1, 1), 50, 0),
+    ("balsara1_lf", (300, 1, 1), 20, 3),
+    ("linwave", (64, 48, 1), 2, 2),
+])
+def test_engine_matches_oracle(cfg, n, steps, seed):
+    e, s = _oracle_case(cfg, n, steps, seed)
+    assert_same(e, s, n)
+
+
+def test_steps_in_one_call_equal_steps_one_by_one():
+    e1, s = _oracle_case("linwave", (16, 12, 10), 4, 1)
+    e2, _ = _oracle_case("linwave", (16, 12, 10), 4, 1, split=True)
+    assert np.array_equal(e1.download(), e2.download())
+    assert np.array_equal(e1.download(), s["p"])
