@@ -77,6 +77,16 @@ CONFIGS = {
                 dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)",
                      RECON_TYPE_CHOICE="(RECON_PPM_MC)", FLUX_TYPE_CHOICE="(FLUX_HLLE)"),
                 []),
+    # Entropy-equation fix off: the inversion tree without pow(), so every
+    # branch of it can be compared bit for bit with a GPU build.
+    "balsara1_noee": ("init.balsara1.c",
+                      dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_OUTFLOW)", RECON_TYPE_CHOICE="(RECON_MC)",
+                           FLUX_TYPE_CHOICE="(FLUX_HLLE)", USE_ENTROPY_EQ="(0)"),
+                      [("cour = 0.8 ;", "cour = 0.5 ;")]),
+    "linwave_noee": ("init.linearwave.c",
+                     dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)", RECON_TYPE_CHOICE="(RECON_PPM_MC)",
+                          FLUX_TYPE_CHOICE="(FLUX_HLLE)", USE_ENTROPY_EQ="(0)"),
+                     []),
     # Same setup with van Leer PPM limiter and LF flux.
     "linwave_vl": ("init.linearwave.c",
                    dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)",

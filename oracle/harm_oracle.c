@@ -20,6 +20,13 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* Test hook: tests/test_pow_sensitivity.py rebuilds the oracle with
+ * -DOR_POW_HOOK=<function> to perturb every pow() result. */
+#ifdef OR_POW_HOOK
+double OR_POW_HOOK(double, double);
+#define pow OR_POW_HOOK
+#endif
+
 #define NP 8
 #define NG 3
 #define NDIM 4

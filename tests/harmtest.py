@@ -26,6 +26,8 @@ CONFIG_SWITCHES = {
     "balsara1_lf": dict(recon=0, flux=0, ct_para=0, bc=0, metric_dim=0, ee=1, cooling=0, rescale=0),
     "linwave": dict(recon=5, flux=1, ct_para=1, bc=1, metric_dim=0, ee=1, cooling=0, rescale=0),
     "linwave_vl": dict(recon=4, flux=0, ct_para=1, bc=1, metric_dim=0, ee=1, cooling=0, rescale=0),
+    "balsara1_noee": dict(recon=2, flux=1, ct_para=1, bc=0, metric_dim=0, ee=0, cooling=0, rescale=0),
+    "linwave_noee": dict(recon=5, flux=1, ct_para=1, bc=1, metric_dim=0, ee=0, cooling=0, rescale=0),
 }
 
 
