@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libharmgpu.so")
+LIB_PATH = os.environ.get("HARMGPU_LIB") or os.path.join(HERE, "libharmgpu.so")
 NG, NP, NFAIL, NGEOM = 3, 8, 15, 42
 
 # options.h switch values accepted by the engine

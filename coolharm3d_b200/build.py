@@ -36,14 +36,15 @@ def up_to_date():
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
-def build(force=False, verbose=False):
-    if not force and up_to_date():
+def build(force=False, verbose=False, out=None, defines=()):
+    lib = out or LIB
+    if not force and out is None and up_to_date():
         return LIB
     objs = []
     procs = []
     for s in SOURCES:
         o = os.path.join(CSRC, s.replace(".cu", ".o"))
-        cmd = [nvcc()] + flags() + ["-c", os.path.join(CSRC, s), "-o", o]
+        cmd = [nvcc()] + flags() + ["-D" + d for d in defines] + ["-c", os.path.join(CSRC, s), "-o", o]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((subprocess.Popen(cmd), s))
@@ -51,12 +52,12 @@ def build(force=False, verbose=False):
     for p, s in procs:
         if p.wait() != 0:
             raise RuntimeError("nvcc failed on " + s)
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     subprocess.check_call([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs)
-    os.replace(tmp, LIB)
+    os.replace(tmp, lib)
     for o in objs:
         os.remove(o)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

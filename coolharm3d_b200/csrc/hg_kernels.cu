@@ -26,6 +26,9 @@
 namespace hg {
 
 #define HG_BLK 128
+#ifndef HG_FLUX_MINB
+#define HG_FLUX_MINB 4
+#endif
 
 __device__ __forceinline__ int rs_type(int l) { return l == RHO ? 0 : (l == UU ? 2 : 1); }
 
@@ -50,7 +53,9 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long *d
   if (threadIdx.x == 0) {
     double m = red[0];
     for (int w = 1; w < HG_BLK / 32; w++) m = red[w] > m ? red[w] : m;
-    if (m > 0.) atomicMax(dst, (unsigned long long)__double_as_longlong(m));
+    // the maximum only grows: skip the atomic when it cannot raise it
+    if (m > 0. && m > __longlong_as_double((long long)*(volatile unsigned long long *)dst))
+      atomicMax(dst, (unsigned long long)__double_as_longlong(m));
   }
 }
 
@@ -157,13 +162,70 @@ __device__ __forceinline__ void face_prims(const GridDev &G, const double *__res
 
 // ---------------------------------------------------------------------------
 // k_flux: F[d] on faces [lo, lo+n) (reference indices).
-template <bool RS>
-__global__ void __launch_bounds__(HG_BLK) k_flux(GridDev G, const double *__restrict__ ph, int d, int lo0, int lo1,
-                                                 int lo2, int n0, int n1, int n2, unsigned int mult)
+// One component of primtoflux(pr, q, dir) (phys.c:28-63), same operations.
+__device__ __forceinline__ double flux_comp(const double *pr, const State &q, int dir, double gg, int l)
+{
+  const double eta_ucon = q.eta * q.ucon[dir];
+  const double bcon_dir = q.bcon[dir];
+  double f;
+  if (l == RHO) {
+    f = pr[RHO] * q.ucon[dir];
+  } else if (l <= U3) {
+    const int a = l - 1;  // UU -> 0, U1 -> 1, ...
+    double m = eta_ucon * q.ucov[a] - bcon_dir * q.bcov[a];
+    if (a == dir) m += q.ptot;
+    f = (l == UU) ? m + pr[RHO] * q.ucon[dir] : m;
+  } else {
+    const int a = l - 4;
+    f = q.bcon[a] * q.ucon[dir] - q.bcon[dir] * q.ucon[a];
+  }
+  return f * gg;
+}
+
+// HLL/LF flux of a face from its two states; writes the 8 components and
+// returns ctop.  Component by component, so no 32-value temporaries.
+__device__ __forceinline__ double face_flux(const GridDev &G, const double *pl, const double *pr, const Geom &g, int d,
+                                            int i, int j, int k, unsigned int mult, double *__restrict__ Fd, long o)
+{
+  const int dim = d + 1;
+  State ql, qr;
+  if (get_state(pl, g, G.gam, ql)) book_face(G, i, j, k, mult);
+  if (get_state(pr, g, G.gam, qr)) book_face(G, i, j, k, mult);
+  double cmaxl, cminl, cmaxr, cminr;
+  vchar_fast(ql, g, dim, G.gam, &cmaxl, &cminl);
+  vchar_fast(qr, g, dim, G.gam, &cmaxr, &cminr);
+  const double a0 = 0. > cmaxl ? 0. : cmaxl;
+  const double cmax = fabs(a0 > cmaxr ? a0 : cmaxr);
+  const double a1 = 0. > -cminl ? 0. : -cminl;
+  const double cmin = fabs(a1 > -cminr ? a1 : -cminr);
+  const double ctop = cmin > cmax ? cmin : cmax;
+  const double gg = g.g;
+  if (G.flux == 1) {
+    const double den = cmax + cmin + HG_SMALL;
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) {
+      const double Ul = flux_comp(pl, ql, 0, gg, l), Ur = flux_comp(pr, qr, 0, gg, l);
+      const double Fl = flux_comp(pl, ql, dim, gg, l), Fr = flux_comp(pr, qr, dim, gg, l);
+      Fd[l * G.S + o] = (cmax * Fl + cmin * Fr - cmax * cmin * (Ur - Ul)) / den;
+    }
+  } else {
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) {
+      const double Ul = flux_comp(pl, ql, 0, gg, l), Ur = flux_comp(pr, qr, 0, gg, l);
+      const double Fl = flux_comp(pl, ql, dim, gg, l), Fr = flux_comp(pr, qr, dim, gg, l);
+      Fd[l * G.S + o] = 0.5 * (Fl + Fr - ctop * (Ur - Ul));
+    }
+  }
+  return ctop;
+}
+
+// ---------------------------------------------------------------------------
+// k_flux: F[d] on faces [lo, lo+n) (reference indices), one thread per face.
+template <bool RS, int MDIM, int d>
+__global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux(const __grid_constant__ GridDev G, const double *__restrict__ ph,
+                                                 int lo0, int lo1, int lo2, int n0, int n1, int n2, unsigned int mult)
 {
   const long total = (long)n0 * n1 * n2;
-  const int dim = d + 1;
-  double *__restrict__ Fd = G.F[d];
   double vmax = 0.;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const int i = lo0 + (int)(t % n0);
@@ -171,37 +233,18 @@ __global__ void __launch_bounds__(HG_BLK) k_flux(GridDev G, const double *__rest
     const int k = lo2 + (int)(t / ((long)n0 * n1));
     double pl[HG_NPR], pr[HG_NPR];
     face_prims<RS>(G, ph, d, i, j, k, pl, pr);
-    Geom g;
-    load_geom(G, d, i, j, g);
-    State ql, qr;
-    if (get_state(pl, g, G.gam, ql)) book_face(G, i, j, k, mult);
-    if (get_state(pr, g, G.gam, qr)) book_face(G, i, j, k, mult);
-    double Ul[HG_NPR], Ur[HG_NPR], Fl[HG_NPR], Fr[HG_NPR];
-    primtoflux(pl, ql, 0, g, Ul);
-    primtoflux(pr, qr, 0, g, Ur);
-    primtoflux(pl, ql, dim, g, Fl);
-    primtoflux(pr, qr, dim, g, Fr);
-    double cmaxl, cminl, cmaxr, cminr;
-    vchar_fast(ql, g, dim, G.gam, &cmaxl, &cminl);
-    vchar_fast(qr, g, dim, G.gam, &cmaxr, &cminr);
-    const double a0 = 0. > cmaxl ? 0. : cmaxl;
-    const double cmax = fabs(a0 > cmaxr ? a0 : cmaxr);
-    const double a1 = 0. > -cminl ? 0. : -cminl;
-    const double cmin = fabs(a1 > -cminr ? a1 : -cminr);
-    const double ctop = cmin > cmax ? cmin : cmax;
+    double ctop;
+    if (MDIM == 0) {
+      ctop = face_flux(G, pl, pr, G.g0, d, i, j, k, mult, G.F[d], off3(G, i, j, k));
+    } else {
+      Geom g;
+      load_geom(G, d, i, j, g);
+      ctop = face_flux(G, pl, pr, g, d, i, j, k, mult, G.F[d], off3(G, i, j, k));
+    }
     if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
       if (ctop > vmax) vmax = ctop;
-    const long o = off3(G, i, j, k);
-    if (G.flux == 1) {
-      const double den = cmax + cmin + HG_SMALL;
-#pragma unroll
-      for (int l = 0; l < HG_NPR; l++) Fd[l * G.S + o] = (cmax * Fl[l] + cmin * Fr[l] - cmax * cmin * (Ur[l] - Ul[l])) / den;
-    } else {
-#pragma unroll
-      for (int l = 0; l < HG_NPR; l++) Fd[l * G.S + o] = 0.5 * (Fl[l] + Fr[l] - ctop * (Ur[l] - Ul[l]));
-    }
   }
-  block_max_atomic(vmax, &G.sc->maxs[dim]);
+  block_max_atomic(vmax, &G.sc->maxs[d + 1]);
 }
 
 // ---------------------------------------------------------------------------
@@ -328,9 +371,9 @@ __device__ __forceinline__ void update_zone(const GridDev &G, int i, int j, int 
 }
 
 // k_update: every physical zone.  sub = 0 predictor (p_f = ph), 1 corrector (p_f = p).
-template <bool RS>
-__global__ void __launch_bounds__(HG_BLK) k_update(GridDev G, int sub, double dtfac, const double *__restrict__ p_h,
-                                                   double *__restrict__ p_f)
+template <bool RS, int MDIM>
+__global__ void __launch_bounds__(HG_BLK) k_update(const __grid_constant__ GridDev G, int sub, double dtfac,
+                                                   const double *__restrict__ p_h, double *__restrict__ p_f)
 {
   const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
   const long total = (long)N0 * N1 * N2;
@@ -344,8 +387,9 @@ __global__ void __launch_bounds__(HG_BLK) k_update(GridDev G, int sub, double dt
     const int j = HG_NGH + (int)((t / N0) % N1);
     const int k = HG_NGH + (int)(t / ((long)N0 * N1));
     const long o = off3(G, i, j, k);
-    Geom g;
-    load_geom(G, 3, i, j, g);
+    Geom gl;
+    if (MDIM != 0) load_geom(G, 3, i, j, gl);
+    const Geom &g = (MDIM == 0) ? G.g0 : gl;
     double pi[HG_NPR], U[HG_NPR], dU[HG_NPR], pg[HG_NPR];
 #pragma unroll
     for (int l = 0; l < HG_NPR; l++) {
@@ -849,10 +893,20 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
       }
     }
     mark(R, KC_FLUX, s);
-    if (G.rescale)
-      k_flux<true><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, d, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult);
-    else
-      k_flux<false><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, d, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult);
+#define HG_FLUX(RSV, MD, DD) k_flux<RSV, MD, DD><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
+#define HG_FLUX_D(RSV, MD) \
+  if (d == 0) HG_FLUX(RSV, MD, 0); \
+  else if (d == 1) HG_FLUX(RSV, MD, 1); \
+  else HG_FLUX(RSV, MD, 2);
+    if (G.mdim == 0) {
+      if (G.rescale) { HG_FLUX_D(true, 0) }
+      else { HG_FLUX_D(false, 0) }
+    } else {
+      if (G.rescale) { HG_FLUX_D(true, 2) }
+      else { HG_FLUX_D(false, 2) }
+    }
+#undef HG_FLUX_D
+#undef HG_FLUX
   }
   {
     int lo[3], n[3];
@@ -864,8 +918,13 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
     k_emf<<<L.grid_emf, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2]);
   }
   mark(R, KC_UPDATE, s);
-  if (G.rescale) k_update<true><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
-  else k_update<false><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  if (G.mdim == 0) {
+    if (G.rescale) k_update<true, 0><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+    else k_update<false, 0><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  } else {
+    if (G.rescale) k_update<true, 2><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+    else k_update<false, 2><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  }
   mark(R, KC_FALLBACK, s);
   if (G.rescale) k_fallback<true><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
   else k_fallback<false><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
