@@ -44,7 +44,7 @@ class GridDesc(ctypes.Structure):
 EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", "hg_download_prims",
            "hg_upload_prims_tree", "hg_download_prims_tree", "hg_set_time", "hg_step", "hg_get_fail_counts",
            "hg_download_pflag", "hg_download_gamma", "hg_download_nfail", "hg_get_diag", "hg_last_step_ms",
-           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times"]
+           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 _lib = None
@@ -77,6 +77,7 @@ def load_library(path=LIB_PATH):
     lib.hg_build_geometry_minkowski.argtypes = [ctypes.POINTER(GridDesc), P, P]
     lib.hg_profile.argtypes = [P, ctypes.c_int32]
     lib.hg_kernel_times.argtypes = [P, P, P]
+    lib.hg_face_flux.argtypes = [P, ctypes.c_int32, P, P]
     for fn in EXPORTS:
         if fn not in ("hg_destroy", "hg_strerror"):
             getattr(lib, fn).restype = I
@@ -197,6 +198,13 @@ class Engine:
         v = np.empty((NFAIL,) + self.shape, np.int32)
         _check(self.lib.hg_download_nfail(self.h, _ptr(v)), "hg_download_nfail")
         return v
+
+    def face_flux(self, d):
+        """(flux of direction d in the reference layout, max char speed)."""
+        f = np.empty(self.shape + (NP,))
+        m = ctypes.c_double()
+        _check(self.lib.hg_face_flux(self.h, d, _ptr(f), ctypes.byref(m)), "hg_face_flux")
+        return f, m.value
 
     def diag(self):
         m = ctypes.c_double()

@@ -18,6 +18,7 @@
 
 namespace hg {
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R);
+void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d);
 }  // namespace hg
 
 using hg::GridDev;
@@ -428,6 +429,50 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
   if (sc.err) return HG_ERR_DEVICE;
   if (t) *t = sc.t;
   if (dt) *dt = sc.dt;
+  return HG_OK;
+}
+
+extern "C" int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max_char_speed)
+{
+  if (!h || dir < 0 || dir > 2 || !flux) return HG_ERR_BADARG;
+  if (!h->have_geom || !h->have_cells || !h->have_prims) return HG_ERR_STATE;
+  GridDev &G = h->G;
+  HG_CK(cudaSetDevice(h->d.device));
+  HG_CK(cudaMemsetAsync(G.F[dir], 0, sizeof(double) * HG_NPR * G.S, h->stream));
+  hg::launch_face_flux(G, h->L, h->stream, dir);
+  HG_CK(cudaGetLastError());
+  HG_CK(cudaStreamSynchronize(h->stream));
+  // per-cell planes -> reference layout with the variable index innermost
+  std::vector<double> tmp((size_t)HG_NPR * G.S);
+  HG_CK(cudaMemcpy(tmp.data(), G.F[dir], sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
+  // faces numerical_flux() computes (step_ch.c:668-675), in reference indices
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; a++) {
+    if (a == dir) {
+      lo[a] = HG_NGH;
+      hi[a] = G.NE[a] + 1;
+    } else if (G.ct_para) {
+      lo[a] = 0;
+      hi[a] = G.NE[a] + HG_NGH;
+    } else {
+      lo[a] = HG_NGH - 1;
+      hi[a] = G.NE[a] + 1;
+    }
+  }
+  for (int i = 0; i < h->NT[0]; i++)
+    for (int j = 0; j < h->NT[1]; j++)
+      for (int k = 0; k < h->NT[2]; k++) {
+        const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+        double *dst = flux + (((long)i * h->NT[1] + j) * h->NT[2] + k) * HG_NPR;
+        const bool in = i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
+        for (int l = 0; l < HG_NPR; l++) dst[l] = in ? tmp[l * G.S + o] : 0.;
+      }
+  if (max_char_speed) {
+    unsigned long long m;
+    HG_CK(cudaMemcpy(&m, sc_field(G, offsetof(hg::DevScalars, maxs) + sizeof(unsigned long long) * (dir + 1)),
+                     sizeof(m), cudaMemcpyDeviceToHost));
+    memcpy(max_char_speed, &m, sizeof(double));
+  }
   return HG_OK;
 }
 

@@ -866,14 +866,9 @@ static inline void mark(EventRec *r, int cls, cudaStream_t s)
   r->n++;
 }
 
-static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int sub, EventRec *R)
+static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, int d,
+                            EventRec *R)
 {
-  const double *ph = sub == 0 ? G.p : G.ph;
-  double *pf = sub == 0 ? G.ph : G.p;
-  const double dtfac = sub == 0 ? 0.5 : 1.0;
-  mark(R, KC_MISC, s);
-  k_begin<<<1, 1, 0, s>>>(G.sc);
-  for (int d = 0; d < 3; d++) {
     int lo[3], n[3];
     unsigned int mult = 1;
     for (int a = 0; a < 3; a++) {
@@ -907,7 +902,16 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
     }
 #undef HG_FLUX_D
 #undef HG_FLUX
-  }
+}
+
+static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int sub, EventRec *R)
+{
+  const double *ph = sub == 0 ? G.p : G.ph;
+  double *pf = sub == 0 ? G.ph : G.p;
+  const double dtfac = sub == 0 ? 0.5 : 1.0;
+  mark(R, KC_MISC, s);
+  k_begin<<<1, 1, 0, s>>>(G.sc);
+  for (int d = 0; d < 3; d++) launch_flux_dir(G, L, s, ph, d, R);
   {
     int lo[3], n[3];
     for (int a = 0; a < 3; a++) {
@@ -936,6 +940,15 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
   k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, pf, 1);
 }
 
+__global__ void k_reset_max(DevScalars *sc, int dim) { sc->maxs[dim] = 0ull; }
+
+// Fluxes of direction d from the resident primitives G.p (hg_face_flux).
+void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d)
+{
+  k_reset_max<<<1, 1, 0, s>>>(G.sc, d + 1);
+  launch_flux_dir(G, L, s, G.p, d, nullptr);
+}
+
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R)
 {
   launch_substep(G, L, s, 0, R);
@@ -946,3 +959,4 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
 }
 
 }  // namespace hg
+

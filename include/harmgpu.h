@@ -113,6 +113,14 @@ int hg_download_pflag(hg_handle *h, int32_t *pflag);
 int hg_download_gamma(hg_handle *h, double *p_gamma);
 int hg_download_nfail(hg_handle *h, int32_t *nfail);
 
+/* Numerical fluxes of direction dir (0, 1, 2 = x1, x2, x3) of the resident
+ * primitives: the HLL/LF fluxes numerical_flux() computes (step_ch.c:636-790,
+ * before flux_ct) on every face it computes, at the lower face of each cell,
+ * in the reference layout (N1TOT x N2TOT x N3TOT x 8; other faces 0), and
+ * the maximum characteristic speed over physical faces (step_ch.c:716-724).
+ * diag()'s boundary-flux diagnostics (diag.c:704-815) read these fluxes. */
+int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max_char_speed);
+
 /* Diagnostics of the last step: M_tot (sum of U[RHO] over the domain after
  * the corrector, step_ch.c:402) and the per-direction maximum
  * characteristic speeds that set dx[0] (step_ch.c:716-724). */

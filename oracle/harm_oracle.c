@@ -1694,6 +1694,17 @@ void or_get_time(const or_ctx *c, double *t, double *dt, double *m)
 }
 long or_ntot(const or_ctx *c) { return c->ntot; }
 
+void or_face_flux(or_ctx *c, int d, double *flux, double *mcs)
+{
+  memset(c->F, 0, sizeof(double) * c->ntot * 3 * NP);
+  memcpy(c->ph, c->p, sizeof(double) * c->ntot * NP);
+  reconstruct_fast(c, c->ph);
+  numerical_flux(c);
+  for (long id = 0; id < c->ntot; id++)
+    for (int l = 0; l < NP; l++) flux[id * NP + l] = FX(c, id, d, l);
+  *mcs = c->max_char_speed[d + 1];
+}
+
 void or_step(or_ctx *c, int nsteps)
 {
   for (int s = 0; s < nsteps; s++) step_ch(c);

@@ -143,6 +143,7 @@ def oracle_lib():
             getattr(lib, fn).argtypes = [P, P]
         lib.or_get_time.argtypes = [P, P, P, P]
         lib.or_step.argtypes = [P, ctypes.c_int]
+        lib.or_face_flux.argtypes = [P, ctypes.c_int, P, P]
         lib.or_ntot.restype = ctypes.c_long
         lib.or_ntot.argtypes = [P]
         _olib = lib
@@ -185,6 +186,12 @@ class Oracle:
 
     def step(self, n=1):
         self.lib.or_step(self.h, n)
+
+    def face_flux(self, d):
+        f = np.empty(self.shape + (NP,))
+        m = ctypes.c_double()
+        self.lib.or_face_flux(self.h, d, _ptr(f), ctypes.byref(m))
+        return f, m.value
 
     def state(self):
         ncell = self.shape[0] * self.shape[1] * self.shape[2]
