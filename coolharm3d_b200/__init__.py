@@ -44,7 +44,7 @@ class GridDesc(ctypes.Structure):
 EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", "hg_download_prims",
            "hg_upload_prims_tree", "hg_download_prims_tree", "hg_set_time", "hg_step", "hg_get_fail_counts",
            "hg_download_pflag", "hg_download_gamma", "hg_download_nfail", "hg_get_diag", "hg_last_step_ms",
-           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux"]
+           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 _lib = None
@@ -78,6 +78,7 @@ def load_library(path=LIB_PATH):
     lib.hg_profile.argtypes = [P, ctypes.c_int32]
     lib.hg_kernel_times.argtypes = [P, P, P]
     lib.hg_face_flux.argtypes = [P, ctypes.c_int32, P, P]
+    lib.hg_face_flux_noalloc.argtypes = [ctypes.POINTER(GridDesc), P, P, P, P, ctypes.c_int32, P]
     for fn in EXPORTS:
         if fn not in ("hg_destroy", "hg_strerror"):
             getattr(lib, fn).restype = I

@@ -21,6 +21,9 @@
 // per block and deterministic.
 #include <cuda_runtime.h>
 
+#include <cstdio>
+#include <cstring>
+
 #include "hg_fallback.cuh"
 
 namespace hg {
@@ -960,3 +963,201 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
 
 }  // namespace hg
 
+// ===========================================================================
+// hg_face_flux_noalloc: hg_face_flux for callers that cannot allocate device
+// memory.  Its only scratch -- the per-block maxima of the characteristic
+// speed and a completion counter -- lives in the file-scope array below, so
+// every GPU that loads the library holds it (256 KiB + 256 B) until exit.
+// Host code never dereferences hg_na_scratch: it is a host-side stand-in for
+// the symbol, and a kernel given its host address would fault or read the
+// wrong memory.  The device address is looked up once per device with
+// cudaGetSymbolAddress on the first call made with that device current.
+// ===========================================================================
+namespace hg {
+
+#define HG_NA_MAX_BLOCKS 32768  // one block per 128 faces: at most 4,194,304 faces per call
+static __device__ __align__(256) unsigned long long hg_na_scratch[HG_NA_MAX_BLOCKS + 32];
+static unsigned long long *hg_na_dev_ptr[64];  // device address of hg_na_scratch, per device ordinal
+
+// face_flux() without the failure bookkeeping (the caller gets fluxes only).
+__device__ __forceinline__ double face_flux_na(const GridDev &G, const double *pl, const double *pr, const Geom &g,
+                                               int d, double *__restrict__ Fd, long o)
+{
+  const int dim = d + 1;
+  State ql, qr;
+  get_state(pl, g, G.gam, ql);
+  get_state(pr, g, G.gam, qr);
+  double cmaxl, cminl, cmaxr, cminr;
+  vchar_fast(ql, g, dim, G.gam, &cmaxl, &cminl);
+  vchar_fast(qr, g, dim, G.gam, &cmaxr, &cminr);
+  const double a0 = 0. > cmaxl ? 0. : cmaxl;
+  const double cmax = fabs(a0 > cmaxr ? a0 : cmaxr);
+  const double a1 = 0. > -cminl ? 0. : -cminl;
+  const double cmin = fabs(a1 > -cminr ? a1 : -cminr);
+  const double ctop = cmin > cmax ? cmin : cmax;
+  const double gg = g.g;
+#pragma unroll
+  for (int l = 0; l < HG_NPR; l++) {
+    const double Ul = flux_comp(pl, ql, 0, gg, l), Ur = flux_comp(pr, qr, 0, gg, l);
+    const double Fl = flux_comp(pl, ql, dim, gg, l), Fr = flux_comp(pr, qr, dim, gg, l);
+    Fd[l * G.S + o] = (G.flux == 1) ? (cmax * Fl + cmin * Fr - cmax * cmin * (Ur - Ul)) / (cmax + cmin + HG_SMALL)
+                                    : 0.5 * (Fl + Fr - ctop * (Ur - Ul));
+  }
+  return ctop;
+}
+
+// One thread per face, one block per 128 faces; each block leaves its maximum
+// in scratch[block], the last block to finish reduces them.
+template <int d>
+__global__ void __launch_bounds__(HG_BLK) k_flux_noalloc(const __grid_constant__ GridDev G,
+                                                         const double *__restrict__ prims, int lo0, int lo1, int lo2,
+                                                         int n0, int n1, int n2, double *max_out,
+                                                         unsigned long long *scratch)
+{
+  const long total = (long)n0 * n1 * n2;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double vmax = 0.;
+  if (t < total) {
+    const int i = lo0 + (int)(t % n0);
+    const int j = lo1 + (int)((t / n0) % n1);
+    const int k = lo2 + (int)(t / ((long)n0 * n1));
+    double pl[HG_NPR], pr[HG_NPR];
+    face_prims<false>(G, prims, d, i, j, k, pl, pr);
+    const double ctop = face_flux_na(G, pl, pr, G.g0, d, G.F[d], off3(G, i, j, k));
+    if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
+      if (ctop > vmax) vmax = ctop;
+  }
+  __shared__ double red[HG_BLK / 32];
+  __shared__ bool last;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double w = __shfl_down_sync(0xffffffffu, vmax, o);
+    vmax = w > vmax ? w : vmax;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = vmax;
+  __syncthreads();
+  unsigned long long *counter = scratch + HG_NA_MAX_BLOCKS;
+  if (threadIdx.x == 0) {
+    double m = red[0];
+    for (int w = 1; w < HG_BLK / 32; w++) m = red[w] > m ? red[w] : m;
+    scratch[blockIdx.x] = (unsigned long long)__double_as_longlong(m);
+    __threadfence();
+    last = (atomicAdd(counter, 1ull) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double m = 0.;
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    const double v = __longlong_as_double((long long)__ldcg(scratch + b));
+    m = v > m ? v : m;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double w = __shfl_down_sync(0xffffffffu, m, o);
+    m = w > m ? w : m;
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < HG_BLK / 32; w++) m = red[w] > m ? red[w] : m;
+    *max_out = m;
+    *counter = 0ull;  // leave the counter at zero for the next call
+  }
+}
+
+}  // namespace hg
+
+#include <mutex>
+
+#include "harmgpu.h"
+
+extern "C" int hg_face_flux_noalloc(const hg_grid_desc *d, const double *geom, const double *prims, double *flux,
+                                    double *max_char_speed, int32_t dir, void *stream)
+{
+  using namespace hg;
+  if (!d || !geom || !prims || !flux || !max_char_speed || dir < 0 || dir > 2) return HG_ERR_BADARG;
+  if (d->metric_dim != 0 || d->rescale_r != 0 || d->n1 < 2 || d->n2 < 2 || d->n3 < 2) return HG_ERR_BADARG;
+  if (d->recon_type < 0 || d->recon_type > 5 || (d->flux_type != 0 && d->flux_type != 1)) return HG_ERR_BADARG;
+  const int n[3] = {d->n1, d->n2, d->n3};
+  int lo[3], cnt[3];
+  for (int a = 0; a < 3; a++) {  // numerical_flux()'s face ranges (step_ch.c:668-675)
+    if (a == dir) {
+      lo[a] = HG_NGH;
+      cnt[a] = n[a] + 1;
+    } else if (d->use_flux_ct_para) {
+      lo[a] = 0;
+      cnt[a] = n[a] + 2 * HG_NGH;
+    } else {
+      lo[a] = HG_NGH - 1;
+      cnt[a] = n[a] + 2;
+    }
+  }
+  const long faces = (long)cnt[0] * cnt[1] * cnt[2];
+  const long blocks = (faces + HG_BLK - 1) / HG_BLK;
+  if (blocks > HG_NA_MAX_BLOCKS) {
+    fprintf(stderr, "hg_face_flux_noalloc: %ld faces exceed the limit of %d faces per call\n", faces,
+            HG_NA_MAX_BLOCKS * HG_BLK);
+    return HG_ERR_BADARG;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HG_ERR_CUDA;
+  {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!hg_na_dev_ptr[dev]) {
+      void *p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, hg_na_scratch);
+      if (e != cudaSuccess || !p) {
+        fprintf(stderr, "hg_face_flux_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+        return HG_ERR_CUDA;
+      }
+      hg_na_dev_ptr[dev] = (unsigned long long *)p;
+    }
+  }
+  unsigned long long *scratch = hg_na_dev_ptr[dev];
+  // the reference layout: variable innermost, k, j, i outermost
+  GridDev G;
+  memset(&G, 0, sizeof(G));
+  const long st2 = HG_NPR, st1 = st2 * (n[2] + 2 * HG_NGH), st0 = st1 * (n[1] + 2 * HG_NGH);
+  G.st[0] = st0;
+  G.st[1] = st1;
+  G.st[2] = st2;
+  G.S = 1;
+  for (int a = 0; a < 3; a++) {
+    G.N[a] = n[a];
+    G.T[a] = n[a] + 2 * HG_NGH;
+    G.NE[a] = n[a] + HG_NGH - 1;
+  }
+  G.recon = d->recon_type;
+  G.flux = d->flux_type;
+  G.gam = d->gam;
+  G.F[dir] = flux;
+  Geom &g = G.g0;
+  memcpy(g.gcon, geom, 16 * 8);
+  memcpy(g.gcov, geom + 16, 16 * 8);
+  g.g = geom[32];
+  g.g_inv = geom[33];
+  g.alpha = geom[34];
+  for (int a = 0; a < 3; a++) g.beta[a] = geom[35 + a];
+  for (int a = 0; a < 4; a++) g.ncon[a] = geom[38 + a];
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(scratch + HG_NA_MAX_BLOCKS, 0, sizeof(unsigned long long), s) != cudaSuccess)
+    return HG_ERR_CUDA;
+  if (dir == 0)
+    k_flux_noalloc<0><<<(unsigned)blocks, HG_BLK, 0, s>>>(G, prims, lo[0], lo[1], lo[2], cnt[0], cnt[1], cnt[2],
+                                                          max_char_speed, scratch);
+  else if (dir == 1)
+    k_flux_noalloc<1><<<(unsigned)blocks, HG_BLK, 0, s>>>(G, prims, lo[0], lo[1], lo[2], cnt[0], cnt[1], cnt[2],
+                                                          max_char_speed, scratch);
+  else
+    k_flux_noalloc<2><<<(unsigned)blocks, HG_BLK, 0, s>>>(G, prims, lo[0], lo[1], lo[2], cnt[0], cnt[1], cnt[2],
+                                                          max_char_speed, scratch);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "hg_face_flux_noalloc: launch failed: %s\n", cudaGetErrorString(e));
+    return HG_ERR_CUDA;
+  }
+  return HG_OK;
+}

@@ -121,6 +121,25 @@ int hg_download_nfail(hg_handle *h, int32_t *nfail);
  * diag()'s boundary-flux diagnostics (diag.c:704-815) read these fluxes. */
 int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max_char_speed);
 
+/* hg_face_flux without any allocation, for callers that cannot allocate
+ * device memory: code running while a CUDA graph is being captured (where
+ * cudaMalloc is not allowed), hosts whose memory pool already owns the whole
+ * device, and real-time loops that must not take the device-wide
+ * synchronisation cudaMalloc/cudaFree imply.  No counterpart in the
+ * reference.  It needs no handle: prims and flux are device pointers in the
+ * reference layout (N1TOT x N2TOT x N3TOT x 8), max_char_speed a device
+ * pointer to one double, geom the host struct of a metric_dim 0 geometry,
+ * stream a cudaStream_t (NULL: the default stream).  Runs asynchronously on
+ * that stream.  Limits: metric_dim 0, no RESCALE_R, every N > 1, and at most
+ * 4,194,304 faces in direction dir (HG_ERR_BADARG beyond).  Its scratch is a
+ * 256 KiB array inside the library, held on every device that loads the
+ * library until exit and shared by all calls: calls that overlap on the GPU
+ * (e.g. on two streams) race and must be serialised by the caller.  The
+ * first call on a device looks up that array's device address, so make the
+ * first call on each device before any stream capture begins. */
+int hg_face_flux_noalloc(const hg_grid_desc *desc, const double *geom, const double *prims, double *flux,
+                         double *max_char_speed, int32_t dir, void *stream);
+
 /* Diagnostics of the last step: M_tot (sum of U[RHO] over the domain after
  * the corrector, step_ch.c:402) and the per-direction maximum
  * characteristic speeds that set dx[0] (step_ch.c:716-724). */
