@@ -44,7 +44,7 @@ class GridDesc(ctypes.Structure):
 EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", "hg_download_prims",
            "hg_upload_prims_tree", "hg_download_prims_tree", "hg_set_time", "hg_step", "hg_get_fail_counts",
            "hg_download_pflag", "hg_download_gamma", "hg_download_nfail", "hg_get_diag", "hg_last_step_ms",
-           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc"]
+           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc", "hg_set_cooling_tables"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 _lib = None
@@ -78,6 +78,7 @@ def load_library(path=LIB_PATH):
     lib.hg_profile.argtypes = [P, ctypes.c_int32]
     lib.hg_kernel_times.argtypes = [P, P, P]
     lib.hg_face_flux.argtypes = [P, ctypes.c_int32, P, P]
+    lib.hg_set_cooling_tables.argtypes = [P, P, P]
     lib.hg_face_flux_noalloc.argtypes = [ctypes.POINTER(GridDesc), P, P, P, P, ctypes.c_int32, P]
     for fn in EXPORTS:
         if fn not in ("hg_destroy", "hg_strerror"):
@@ -160,6 +161,11 @@ class Engine:
         rface = None if rface is None else np.ascontiguousarray(rface, np.float64)
         self._keep = (cell6, rface)
         _check(self.lib.hg_set_cell_data(self.h, _ptr(cell6), _ptr(rface)), "hg_set_cell_data")
+
+    def set_cooling_tables(self, omega, t_target):
+        om = np.ascontiguousarray(omega, np.float64)
+        tt = np.ascontiguousarray(t_target, np.float64)
+        _check(self.lib.hg_set_cooling_tables(self.h, _ptr(om), _ptr(tt)), "hg_set_cooling_tables")
 
     def upload(self, p):
         p = np.ascontiguousarray(p, np.float64)

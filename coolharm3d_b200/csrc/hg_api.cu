@@ -30,7 +30,7 @@ struct hg_handle {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
-  bool have_geom = false, have_cells = false, have_prims = false;
+  bool have_geom = false, have_cells = false, have_prims = false, have_cool = false;
   std::vector<void *> allocs;
   double *h_stage = nullptr;  // pinned staging buffer, 8 planes
   long ntot_ref = 0;          // N1TOT*N2TOT*N3TOT of the reference layout
@@ -88,9 +88,11 @@ static int validate(const hg_grid_desc *d)
     return HG_ERR_BADARG;
   if (d->recon_type < 0 || d->recon_type > 5) return HG_ERR_BADARG;
   if (d->flux_type != 0 && d->flux_type != 1) return HG_ERR_BADARG;
-  if (d->bc_type != 0 && d->bc_type != 1) return HG_ERR_BADARG;
+  if (d->bc_type != 0 && d->bc_type != 1 && d->bc_type != 10) return HG_ERR_BADARG;
+  // the spherical boundaries need the radial and polar directions resolved
+  if (d->bc_type == 10 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
   if (d->metric_dim != 0 && d->metric_dim != 2) return HG_ERR_BADARG;
-  if (d->cooling != 0) return HG_ERR_BADARG;
+  if (d->cooling != 0 && d->cooling != 1) return HG_ERR_BADARG;
   if (d->precision != HG_PREC_FP64) return HG_ERR_BADARG;
   // the tables of METRIC_DIM 2 vary with i and j: those directions must be resolved
   if (d->metric_dim == 2 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
@@ -172,6 +174,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
       ALLOC(G.conn, sizeof(double) * 64 * G.T[0] * G.T[1]);
     }
     if (G.rescale) ALLOC(G.rsc, sizeof(double) * 12 * G.T[0]);
+    if (G.cooling) ALLOC(G.cool, sizeof(double) * 2 * G.T[0]);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device);
     auto grid_for = [&](long work, int per_sm) {
@@ -312,6 +315,22 @@ extern "C" int hg_set_cell_data(hg_handle *h, const double *cell6, const double 
   return HG_OK;
 }
 
+extern "C" int hg_set_cooling_tables(hg_handle *h, const double *omega, const double *t_target)
+{
+  if (!h || !omega || !t_target) return HG_ERR_BADARG;
+  if (!h->G.cooling) return HG_ERR_STATE;
+  HG_CK(cudaSetDevice(h->d.device));
+  const int T0 = h->G.T[0];
+  std::vector<double> c((size_t)2 * T0);
+  for (int i = 0; i < T0; i++) {
+    c[i] = omega[i];
+    c[T0 + i] = t_target[i];
+  }
+  HG_CK(cudaMemcpy(h->G.cool, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+  h->have_cool = true;
+  return HG_OK;
+}
+
 template <class GET>
 static int upload_impl(hg_handle *h, GET get)
 {
@@ -391,6 +410,7 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
 {
   if (!h || nsteps < 0) return HG_ERR_BADARG;
   if (!h->have_geom || !h->have_cells || !h->have_prims) return HG_ERR_STATE;
+  if (h->G.cooling && !h->have_cool) return HG_ERR_STATE;
   HG_CK(cudaSetDevice(h->d.device));
   hg::EventRec rec, *R = nullptr;
   if (h->prof) {

@@ -71,7 +71,8 @@ struct GridDev {
   double *geomT;             // metric_dim 2: 42 planes of HG_NPOS*T0*T1, index (pos*T1 + j)*T0 + i
   long gS;                   // geometry plane size
   double *conn;              // metric_dim 2: 64 planes of T0*T1 (physical i,j only used)
-  double *rsc;               // RESCALE_R: 9 planes of T0: rscale[0..5], and 1/rscale[0..2]
+  double *rsc;               // RESCALE_R: 12 planes of T0: rscale[0..5], 1/rscale[0..5]
+  double *cool;              // cooling 1: 2 planes of T0: Omega(r_i), T(r_i)
   DevScalars *sc;
   unsigned long long *q_idx; // fallback queue: packed (i,j,k)
   double *q_U;               // 8 doubles per queued cell

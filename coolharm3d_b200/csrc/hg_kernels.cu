@@ -237,12 +237,18 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux(const __grid_cons
     double pl[HG_NPR], pr[HG_NPR];
     face_prims<RS>(G, ph, d, i, j, k, pl, pr);
     double ctop;
+    const long o = off3(G, i, j, k);
     if (MDIM == 0) {
-      ctop = face_flux(G, pl, pr, G.g0, d, i, j, k, mult, G.F[d], off3(G, i, j, k));
+      ctop = face_flux(G, pl, pr, G.g0, d, i, j, k, mult, G.F[d], o);
     } else {
       Geom g;
       load_geom(G, d, i, j, g);
-      ctop = face_flux(G, pl, pr, g, d, i, j, k, mult, G.F[d], off3(G, i, j, k));
+      ctop = face_flux(G, pl, pr, g, d, i, j, k, mult, G.F[d], o);
+    }
+    if (d == 0 && G.bc == 10) {  // fix_flux(), bounds.c:2263-2275: no mass inflow through r_in, r_out
+      double *fr = G.F[0] + RHO * G.S + o;
+      if (i == HG_NGH && *fr > 0) *fr = 0.;
+      if (i == G.NE[0] + 1 && *fr < 0) *fr = 0.;
     }
     if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
       if (ctop > vmax) vmax = ctop;
@@ -310,8 +316,8 @@ __device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, 
 #pragma unroll
   for (int l = 0; l < HG_NPR; l++) dU[l] = 0.;
   int bad = 0;
+  State q;
   if (G.mdim > 0) {
-    State q;
     bad = get_state(ph, g, G.gam, q);
     double mhd[4][4];
     mhd_row(q, 0, mhd[0]);
@@ -327,6 +333,22 @@ __device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, 
         dU[U1] += mhd[a][b] * __ldg(G.conn + ((b * 4 + 1) * 4 + a) * cS + co);
         dU[U2] += mhd[a][b] * __ldg(G.conn + ((b * 4 + 2) * 4 + a) * cS + co);
       }
+  }
+  if (G.cooling == 1) {  // phys.c:162-172, source_cooling_func phys.c:541-582
+    if (G.mdim == 0) bad = get_state(ph, g, G.gam, q);
+    const int bound = ((q.ucov[0] * (q.p + ph[UU] + ph[RHO] + q.bsq)) > (-ph[RHO])) ? 1 : 0;
+    double f_cool = 0.;
+    if (bound) {  // cooling_func_hr_disk, phys.c:779-783 (s_norm 1, q_exp 1/2)
+      const double T_r = G.cool[G.T[0] + i], Omega_r = G.cool[i];
+      const double E_ratio = (G.gam - 1.) * ph[UU] / (ph[RHO] * T_r);
+      const double dE = E_ratio - 1.;
+      // pow(x, 0.5) of the reference, as the correctly rounded square root
+      f_cool = 1. * ph[UU] * Omega_r * sqrt(dE + fabs(dE));
+    }
+    dU[UU] -= f_cool * q.ucov[0];
+    dU[U1] -= f_cool * q.ucov[1];
+    dU[U2] -= f_cool * q.ucov[2];
+    dU[U3] -= f_cool * q.ucov[3];
   }
   dU[UU] *= g.g;
   dU[U1] *= g.g;
@@ -637,6 +659,74 @@ __device__ __forceinline__ int bc_map(int x, int n, int periodic)
   return x;
 }
 
+// x2 reflection of BC_SPHERICAL_OUTFLOW3 (bounds.c:522-546): ghost N2S-1-g
+// copies N2S+g, ghost N2E+1+g copies N2E-g.
+__device__ __forceinline__ int sph_reflect(int x, int n)
+{
+  const int s = HG_NGH, e = n + HG_NGH - 1;
+  if (x < s) return 2 * s - 1 - x;
+  if (x > e) return 2 * e + 1 - x;
+  return x;
+}
+
+// inflow_check(), bounds.c:2304-2370 (dir = RR, USE_GAMMA_CEILING_X1DN_BC 0).
+// Returns 1 if gamma_calc failed (ucon_calc's FAIL_GAMMA_CALC).
+__device__ __forceinline__ int inflow_check(double *pr, const Geom &g, int type)
+{
+  double gamma;
+  const int bad = gamma_calc(pr, g, &gamma);
+  double ucon[4];
+  ucon[0] = gamma * g.ncon[0];
+  ucon[1] = pr[U1] - ucon[0] * g.beta[0];
+  if (((ucon[1] > 0.) && (type == 0)) || ((ucon[1] < 0.) && (type == 1))) {
+    gamma = g.alpha * ucon[0];
+    pr[U1] /= gamma;
+    pr[U2] /= gamma;
+    pr[U3] /= gamma;
+    pr[U1] = g.beta[0] * g.ncon[0];
+    double vsq = 0.;
+    for (int a = 1; a < 4; a++)
+      for (int b = 1; b < 4; b++) vsq += g.gcov[a][b] * pr[U1 + a - 1] * pr[U1 + b - 1];
+    if (fabs(vsq) < 1.e-13) vsq = fabs(vsq);
+    if (vsq < 0.) vsq = 0.;
+    if (vsq >= 1.) vsq = 1. - 1. / (HG_GAMMAMAX * HG_GAMMAMAX);
+    gamma = 1. / sqrt(1. - vsq);
+    pr[U1] *= gamma;
+    pr[U2] *= gamma;
+    pr[U3] *= gamma;
+  }
+  return bad;
+}
+
+// One ghost zone of BC_SPHERICAL_OUTFLOW3 (bounds.c:492-575).  The reference
+// fills x1 ghosts (copy + inflow_check at the ghost's own geometry) over
+// physical j,k, then x2 ghosts over all i (reflection, U2 and B2 flipped),
+// then x3 ghosts over all i,j (periodic); composed per zone: take the zone
+// the three maps reach, apply inflow_check at (ghost i, reflected j) if i is
+// a ghost, then the flips if j is a ghost.  A gamma failure in inflow_check
+// is booked only where the reference calls it (j and k physical).
+__device__ __forceinline__ void bounds_spherical3(const GridDev &G, double *__restrict__ pa, int i, int j, int k,
+                                                  long od)
+{
+  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
+  const int si = bc_map(i, N0, 0), sj = sph_reflect(j, N1), sk = bc_map(k, N2, 1);
+  const long os = (long)si * G.st[0] + (long)sj * G.st[1] + (long)sk * G.st[2];
+  double v[HG_NPR];
+#pragma unroll
+  for (int l = 0; l < HG_NPR; l++) v[l] = pa[l * G.S + os];
+  if (i != si) {
+    Geom g;
+    load_geom(G, 3, i, sj, g);
+    if (inflow_check(v, g, i > si ? 1 : 0) && j == sj && k == sk) book(G, NF_GAMMA_CALC, i, j, k);
+  }
+  if (j != sj) {
+    v[U2] *= -1;
+    v[B2] *= -1;
+  }
+#pragma unroll
+  for (int l = 0; l < HG_NPR; l++) pa[l * G.S + od] = v[l];
+}
+
 __global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict__ pa, int conditional)
 {
   if (conditional && !G.sc->bnd_phys) return;
@@ -670,10 +760,17 @@ __global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict
       k = HG_NGH + (int)(u / ((long)(T0 - N0) * N1));
     }
     // degenerate directions have no ghosts, so these are reference indices
+    const long od = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+    if (G.bc == 10) {
+      bounds_spherical3(G, pa, i, j, k, od);
+      G.pflag[od] = fl ? G.pflag[(long)bc_map(i, N0, 0) * G.st[0] + (long)sph_reflect(j, N1) * G.st[1] +
+                                 (long)bc_map(k, N2, 1) * G.st[2]]
+                       : 0;
+      continue;
+    }
     const int si = G.deg[0] ? i : bc_map(i, N0, per);
     const int sj = G.deg[1] ? j : bc_map(j, N1, per);
     const int sk = G.deg[2] ? k : bc_map(k, N2, per);
-    const long od = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
     const long os = (long)si * G.st[0] + (long)sj * G.st[1] + (long)sk * G.st[2];
 #pragma unroll
     for (int l = 0; l < HG_NPR; l++) pa[l * S + od] = pa[l * S + os];

@@ -89,6 +89,12 @@ int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom, const doub
  * rface[N1TOT]: x[RR] at FACE1 (RESCALE_R only, else NULL). */
 int hg_set_cell_data(hg_handle *h, const double *cell6, const double *rface);
 
+/* USE_COOLING_FUNCTION 1: per radial index i (N1TOT values each) the orbital
+ * frequency Omega(r_i) and target temperature T(r_i) that
+ * cooling_func_hr_disk() tabulates on its first call (phys.c:683-704,
+ * omega_circular_equatorial() and target_temperature()). */
+int hg_set_cooling_tables(hg_handle *h, const double *omega, const double *t_target);
+
 /* Primitive variables in the reference layout (flattened p[i][j][k][l]).
  * Upload is hg_upload_prims; download is what diag()/restart_write() need. */
 int hg_upload_prims(hg_handle *h, const double *p);

@@ -58,7 +58,8 @@ MINK = {
     "RESCALE_R": "(0)",
 }
 
-# name -> (init file, options.h edits, init-file literal edits)
+# name -> (init file, options.h edits, literal edits to the init file; an edit
+# given as (file, old, new) applies to another staged source file)
 CONFIGS = {
     # Balsara test 1, 1D shock tube: MC + HLLE + para flux-CT, outflow.
     "balsara1": ("init.balsara1.c",
@@ -87,6 +88,24 @@ CONFIGS = {
                      dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)", RECON_TYPE_CHOICE="(RECON_PPM_MC)",
                           FLUX_TYPE_CHOICE="(FLUX_HLLE)", USE_ENTROPY_EQ="(0)"),
                      []),
+    # Fishbone-Moncrief torus in Kerr-Schild a=0.9, modified KS (DIAGONAL3)
+    # coordinates, SPHERICAL_OUTFLOW3, PPM_MC + HLLE, para flux-CT, RESCALE_R,
+    # entropy fix, H/R = 0.1 cooling: the configuration's parameters replace
+    # the shipped ones (a 0 -> 0.9, Rout 40 -> 120, phi range pi/2 -> 2 pi,
+    # Gamma 4/3 -> 5/3, r_in 10 -> 6, r_pmax 16 -> 12, randfact 0 -> 0.04,
+    # USE_COOLING_FUNCTION 5 -> 1, FLUX_LF -> FLUX_HLLE, h_o_r 0.05 -> 0.1),
+    # and the stray ';' after init_prim's header (init.torus.c:355) is removed.
+    "torus": ("init.torus.c",
+              dict(USE_COOLING_FUNCTION="(1)", FLUX_TYPE_CHOICE="(FLUX_HLLE)"),
+              [("gam = (4./3.) ;", "gam = (5./3.) ;"),
+               ("GridLength[3] = M_PI/2. ;", "GridLength[3] = 2.*M_PI ;"),
+               ("  a = 0.;          /* Spin", "  a = 0.9;          /* Spin"),
+               ("Rout     = 40.;", "Rout     = 120.;"),
+               ("struct of_coord *coords, double *pr);\n{", "struct of_coord *coords, double *pr)\n{"),
+               ("rin = 10. ;", "rin = 6. ;"),
+               ("rmax = 16. ;", "rmax = 12. ;"),
+               ("  randfact = 0.;", "  randfact = 4.e-2;"),
+               ("phys.c", "const double h_o_r  = 5.e-2;", "const double h_o_r  = 1.e-1;")]),
     # Same setup with van Leer PPM limiter and LF flux.
     "linwave_vl": ("init.linearwave.c",
                    dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)",
@@ -117,13 +136,13 @@ def stage(cfg):
     for k, v in dict(IO_OFF, **opts).items():
         text = set_define(text, k, v)
     open(opt_path, "w").write(text)
-    ipath = os.path.join(sdir, init_file)
-    itext = open(ipath).read()
-    for old, new in init_edits:
-        if old not in itext:
-            raise SystemExit("build_ref: edit target %r not in %s" % (old, init_file))
-        itext = itext.replace(old, new, 1)
-    open(ipath, "w").write(itext)
+    for e in init_edits:
+        fname, old, new = (init_file,) + tuple(e) if len(e) == 2 else e
+        fpath = os.path.join(sdir, fname)
+        text = open(fpath).read()
+        if old not in text:
+            raise SystemExit("build_ref: edit target %r not in %s" % (old, fname))
+        open(fpath, "w").write(text.replace(old, new, 1))
     # defs.h: same transform as the reference makefile's defs.h rule.
     defs = []
     for line in open(os.path.join(sdir, "globals.h")):

@@ -87,6 +87,8 @@ struct or_ctx {
   double *conn;  /* metric_dim 2: N1*N2*64 */
   double *cell6;
   double *rscale[6];
+  double *cool_omega, *cool_temp; /* Omega_gf, T_r_gf of cooling_func_hr_disk (phys.c:683-704) */
+  int cool_tables_built;          /* cooling_func_hr_disk's local_first_time has been cleared */
   double *p, *ph, *p_old, *pL, *pR, *F, *emf[3], *cgf, *uconL, *uconR, *U0, *Un, *p_gamma;
   int32_t *pflag;
   int32_t *nfail;
@@ -268,13 +270,15 @@ static void vchar_fast(const or_ctx *c, const state_t *q, const geom_t *g, int j
   else { *vmax = vm; *vmin = vp; }
 }
 
-/* source(), phys.c:121-187 (METRIC_DIM 2 contraction; cooling off) */
+/* source(), phys.c:121-187: T^mu_kappa Gamma^kappa_nu mu for METRIC_DIM 2
+ * (U1, U2 only) and the H/R cooling (USE_COOLING_FUNCTION 1), times sqrt(-g).
+ * get_state() runs once, as in the reference. */
 static void source(or_ctx *c, const double *ph, const geom_t *g, int ii, int jj, double *dU)
 {
   int l;
+  state_t q;
   for (l = 0; l < NP; l++) dU[l] = 0.;
   if (c->d.metric_dim > 0) {
-    state_t q;
     double mhd[4][4];
     const double *cn = &c->conn[64L * ((jj - NG) + (long)c->N2 * (ii - NG))];
     get_state(c, ph, g, &q);
@@ -286,6 +290,32 @@ static void source(or_ctx *c, const double *ph, const geom_t *g, int ii, int jj,
         dU[U1] += mhd[i][j] * cn[(j * 4 + 1) * 4 + i];
         dU[U2] += mhd[i][j] * cn[(j * 4 + 2) * 4 + i];
       }
+  }
+  if (c->d.cooling == 1) {
+    if (c->d.metric_dim == 0) get_state(c, ph, g, &q);
+    int bound = ((q.ucov[0] * (q.p + ph[UU] + ph[RHO] + q.bsq)) > (-ph[RHO])) ? 1 : 0;
+    double f_cool = 0.;
+    if (bound) { /* cooling_func_hr_disk, phys.c:649-784 (s_norm 1, q_exp 0.5) */
+      double T_r = c->cool_temp[ii], Omega_r = c->cool_omega[ii];
+      double E_ratio = (c->d.gam - 1.) * ph[UU] / (ph[RHO] * T_r);
+      double dE = E_ratio - 1.;
+      f_cool = 1. * ph[UU] * Omega_r * pow((dE + fabs(dE)), 0.5);
+      if (!c->cool_tables_built) {
+        /* The reference fills its tables on this first call with
+         * get_coord(j, N2S, N3S, ...) for every j (phys.c:683-690), which
+         * leaves icurr/jcurr/kcurr at (N1TOT-1, N2S, N3S): the remaining
+         * fail() bookings of this zone land on that cell. */
+        c->cool_tables_built = 1;
+        c->icur = c->N1T - 1;
+        c->jcur = NG;
+        c->kcur = NG;
+      }
+    }
+    /* source_cooling_func, phys.c:571-575 */
+    dU[UU] -= f_cool * q.ucov[0];
+    dU[U1] -= f_cool * q.ucov[1];
+    dU[U2] -= f_cool * q.ucov[2];
+    dU[U3] -= f_cool * q.ucov[3];
   }
   dU[UU] *= g->g;
   dU[U1] *= g->g;
@@ -1370,6 +1400,15 @@ static void advance(or_ctx *c, double *p_i, double *p_h, double Dt, double *p_f)
   const int e1 = c->N1 + NG - 1, e2 = c->N2 + NG - 1, e3 = c->N3 + NG - 1;
   reconstruct_fast(c, p_h);
   numerical_flux(c);
+  if (c->d.bc_type == 10) { /* fix_flux(), bounds.c:2263-2275 */
+    int j2, k2;
+    for (j2 = 0; j2 < c->N2T; j2++)
+      for (k2 = 0; k2 < c->N3T; k2++) {
+        long lo = IX(c, NG, j2, k2), hi = IX(c, c->N1 + NG, j2, k2);
+        if (FX(c, lo, 0, RHO) > 0) FX(c, lo, 0, RHO) = 0.;
+        if (FX(c, hi, 0, RHO) < 0) FX(c, hi, 0, RHO) = 0.;
+      }
+  }
   flux_ct(c);
   c->M_tot = 0.;
   for (i = NG; i <= e1; i++)
@@ -1411,6 +1450,33 @@ static void copy_cell(or_ctx *c, double *pa, long dst, long src, int flags)
   if (flags) c->pflag[dst] = c->pflag[src];
 }
 
+/* inflow_check(), bounds.c:2304-2370, dir = RR (USE_GAMMA_CEILING_X1DN_BC 0) */
+static void inflow_check(or_ctx *c, double *pr, int ii, int jj, int kk, int type)
+{
+  const int dir = 1;
+  double ucon[4];
+  geom_t *g = G(c, ii, jj, kk, 3);
+  ucon_calc(c, pr, g, ucon);
+  if (((ucon[dir] > 0.) && (type == 0)) || ((ucon[dir] < 0.) && (type == 1))) {
+    double gamma = g->alpha * ucon[0];
+    pr[U1] /= gamma;
+    pr[U2] /= gamma;
+    pr[U3] /= gamma;
+    pr[U1 + dir - 1] = g->beta[dir - 1] * g->ncon[0];
+    double vsq = 0.;
+    int j, k;
+    for (j = 1; j < NDIM; j++)
+      for (k = 1; k < NDIM; k++) vsq += g->gcov[j][k] * pr[U1 + j - 1] * pr[U1 + k - 1];
+    if (fabs(vsq) < 1.e-13) vsq = fabs(vsq);
+    if (vsq < 0.) vsq = 0.;
+    if (vsq >= 1.) vsq = 1. - 1. / (GAMMAMAX * GAMMAMAX);
+    gamma = 1. / sqrt(1. - vsq);
+    pr[U1] *= gamma;
+    pr[U2] *= gamma;
+    pr[U3] *= gamma;
+  }
+}
+
 static void bounds(or_ctx *c, double *pa)
 {
   int i, j, k, g;
@@ -1442,6 +1508,43 @@ static void bounds(or_ctx *c, double *pa)
       copy_cell(c, pa, IX(c, i, j, e3 + 1 + g), IX(c, i, j, per ? NG + g : e3), 0);
     if (fl) for (i = 0; i < c->N1T; i++) for (j = 0; j < c->N2T; j++) for (g = 0; g < NG; g++)
       c->pflag[IX(c, i, j, e3 + 1 + g)] = c->pflag[IX(c, i, j, per ? NG + g : e3)];
+  } else if (c->d.bc_type == 10) { /* BC_SPHERICAL_OUTFLOW3, bounds.c:492-575 */
+    for (g = 0; g < NG; g++) for (j = NG; j <= e2; j++) for (k = NG; k <= e3; k++)
+      copy_cell(c, pa, IX(c, NG - 1 - g, j, k), IX(c, NG, j, k), 0);
+    for (g = 0; g < NG; g++) for (j = NG; j <= e2; j++) for (k = NG; k <= e3; k++)
+      inflow_check(c, &pa[IX(c, NG - 1 - g, j, k) * NP], NG - 1 - g, j, k, 0);
+    if (fl) for (g = 0; g < NG; g++) for (j = NG; j <= e2; j++) for (k = NG; k <= e3; k++)
+      c->pflag[IX(c, NG - 1 - g, j, k)] = c->pflag[IX(c, NG, j, k)];
+    for (g = 0; g < NG; g++) for (j = NG; j <= e2; j++) for (k = NG; k <= e3; k++)
+      copy_cell(c, pa, IX(c, e1 + 1 + g, j, k), IX(c, e1, j, k), 0);
+    for (g = 0; g < NG; g++) for (j = NG; j <= e2; j++) for (k = NG; k <= e3; k++)
+      inflow_check(c, &pa[IX(c, e1 + 1 + g, j, k) * NP], e1 + 1 + g, j, k, 1);
+    if (fl) for (g = 0; g < NG; g++) for (j = NG; j <= e2; j++) for (k = NG; k <= e3; k++)
+      c->pflag[IX(c, e1 + 1 + g, j, k)] = c->pflag[IX(c, e1, j, k)];
+    for (i = 0; i < c->N1T; i++) for (g = 0; g < NG; g++) for (k = NG; k <= e3; k++) {
+      long d = IX(c, i, NG - 1 - g, k);
+      copy_cell(c, pa, d, IX(c, i, NG + g, k), 0);
+      pa[d * NP + U2] *= -1;
+      pa[d * NP + B2] *= -1;
+    }
+    if (fl) for (i = 0; i < c->N1T; i++) for (g = 0; g < NG; g++) for (k = NG; k <= e3; k++)
+      c->pflag[IX(c, i, NG - 1 - g, k)] = c->pflag[IX(c, i, NG + g, k)];
+    for (i = 0; i < c->N1T; i++) for (g = 0; g < NG; g++) for (k = NG; k <= e3; k++) {
+      long d = IX(c, i, e2 + 1 + g, k);
+      copy_cell(c, pa, d, IX(c, i, e2 - g, k), 0);
+      pa[d * NP + U2] *= -1;
+      pa[d * NP + B2] *= -1;
+    }
+    if (fl) for (i = 0; i < c->N1T; i++) for (g = 0; g < NG; g++) for (k = NG; k <= e3; k++)
+      c->pflag[IX(c, i, e2 + 1 + g, k)] = c->pflag[IX(c, i, e2 - g, k)];
+    for (i = 0; i < c->N1T; i++) for (j = 0; j < c->N2T; j++) for (g = 0; g < NG; g++)
+      copy_cell(c, pa, IX(c, i, j, NG - 1 - g), IX(c, i, j, e3 - g), 0);
+    if (fl) for (i = 0; i < c->N1T; i++) for (j = 0; j < c->N2T; j++) for (g = 0; g < NG; g++)
+      c->pflag[IX(c, i, j, NG - 1 - g)] = c->pflag[IX(c, i, j, e3 - g)];
+    for (i = 0; i < c->N1T; i++) for (j = 0; j < c->N2T; j++) for (g = 0; g < NG; g++)
+      copy_cell(c, pa, IX(c, i, j, e3 + 1 + g), IX(c, i, j, NG + g), 0);
+    if (fl) for (i = 0; i < c->N1T; i++) for (j = 0; j < c->N2T; j++) for (g = 0; g < NG; g++)
+      c->pflag[IX(c, i, j, e3 + 1 + g)] = c->pflag[IX(c, i, j, NG + g)];
   } else {
     fprintf(stderr, "harm_oracle: bc_type %d not supported\n", c->d.bc_type);
     abort();
@@ -1662,7 +1765,7 @@ or_ctx *or_create(const or_desc *d, const double *geom, const double *conn, cons
 void or_destroy(or_ctx *c)
 {
   if (!c) return;
-  free(c->geom); free(c->conn); free(c->cell6);
+  free(c->geom); free(c->conn); free(c->cell6); free(c->cool_omega); free(c->cool_temp);
   for (int a = 0; a < 6; a++) free(c->rscale[a]);
   free(c->p); free(c->ph); free(c->p_old); free(c->pL); free(c->pR); free(c->F);
   for (int a = 0; a < 3; a++) free(c->emf[a]);
@@ -1670,6 +1773,16 @@ void or_destroy(or_ctx *c)
   free(c->pflag); free(c->nfail);
   free(c->vec); free(c->dq); free(c->vL); free(c->vR);
   free(c);
+}
+
+void or_set_cooling(or_ctx *c, const double *omega, const double *temp)
+{
+  free(c->cool_omega);
+  free(c->cool_temp);
+  c->cool_omega = malloc(sizeof(double) * c->N1T);
+  c->cool_temp = malloc(sizeof(double) * c->N1T);
+  memcpy(c->cool_omega, omega, sizeof(double) * c->N1T);
+  memcpy(c->cool_temp, temp, sizeof(double) * c->N1T);
 }
 
 void or_set_prims(or_ctx *c, const double *p_aos, double t, double dt)

@@ -56,6 +56,8 @@ typedef struct or_ctx or_ctx;
 or_ctx *or_create(const or_desc *d, const double *geom, const double *conn,
                   const double *cell6, const double *rface);
 void or_destroy(or_ctx *c);
+/* cooling_func_hr_disk's per-i tables Omega(r_i), T(r_i) (N1TOT each). */
+void or_set_cooling(or_ctx *c, const double *omega, const double *temp);
 void or_set_prims(or_ctx *c, const double *p_aos, double t, double dt);
 void or_get_prims(const or_ctx *c, double *p_aos);
 void or_get_pflag(const or_ctx *c, int32_t *pflag);

@@ -30,6 +30,8 @@
 #include <time.h>
 
 extern void ref_step_ch(void);
+extern double omega_circular_equatorial(double r_loc);
+extern double target_temperature(double r_loc, double h_o_r);
 
 static int probe_started = 0;
 static long probe_maxsteps = -1;
@@ -110,7 +112,8 @@ static void load_state(const char *fname)
  *   int32 N_GEOM, N_CONN; then N_GEOM x 42 doubles (struct of_geom order:
  *   gcon[16], gcov[16], g, g_inv, alpha, beta[3], ncon[4]) of time level 0,
  *   N_CONN x 64 doubles of conn[][][][], and per cell (ALL_LOOP order) the
- *   CENT coordinate data: rhoflr, uuflr, r, x[1], x[2], x[3]. */
+ *   CENT coordinate data: rhoflr, uuflr, r, x[1], x[2], x[3]; then per i:
+ *   x[RR] at FACE1, Omega(r_i), T(r_i) (3 doubles). */
 static void dump_geom(const char *fname)
 {
   FILE *f = fopen(fname, "wb");
@@ -142,6 +145,23 @@ static void dump_geom(const char *fname)
     get_coord(i, j, k, CENT, 0, cd);
     double v[6] = {cd->rhoflr, cd->uuflr, cd->r, cd->x[1], cd->x[2], cd->x[3]};
     fwrite(v, 8, 6, f);
+  }
+  /* per radial index: x[RR] at FACE1 (rescale_prims_r, recon.c:1142-1165) and
+   * the H/R cooling tables of cooling_func_hr_disk (phys.c:683-704), for the
+   * h_o_r given in HARM_PROBE_HOR (0 when not given) */
+  const char *hs = getenv("HARM_PROBE_HOR");
+  double hor = hs ? atof(hs) : 0.;
+  for (i = 0; i < N1TOT; i++) {
+    struct of_coord *cd;
+    get_coord(i, N2S, N3S, FACE1, 0, cd);
+    double rf = cd->x[RR];
+    get_coord(i, N2S, N3S, CENT, 0, cd);
+    double v[3] = {rf, 0., 0.};
+    if (hor > 0.) {
+      v[1] = omega_circular_equatorial(cd->x[RR]);
+      v[2] = target_temperature(cd->x[RR], hor);
+    }
+    fwrite(v, 8, 3, f);
   }
   fclose(f);
 }

@@ -23,7 +23,17 @@ def load(name):
     return d
 
 
+def cell6_of(f):
+    """Per-cell (rhoflr, uuflr, r, ...) array with the fields the step reads."""
+    shape = tuple(x + 6 for x in f["n"])
+    c = np.zeros(shape + (6,))
+    c[..., :2] = f["cell_floors"]
+    c[:, :, :, 2] = f["r_line"][:, None, None]
+    return c
+
+
 def geomd(f, cell6=None):
     """Descriptor dict for harmtest.Oracle from a fixture."""
     return dict(gam=f["gam"], cour=f["cour"], grid_length=f["grid_length"], startx=f["startx"], dx=f["dx"],
-                geom=f["geom"], conn=f["conn"], cell6=cell6)
+                geom=f["geom"], conn=f["conn"], cell6=cell6 if cell6 is not None else cell6_of(f),
+                rface=f["rface"], cool_omega=f["cool_omega"], cool_temp=f["cool_temp"])

@@ -39,6 +39,12 @@ CASES = [
     # entropy fix on, one step: pow() differs by ulps between glibc and CUDA
     ("balsara1_stress_n64_s1", "balsara1", (64, 1, 1), 1, 11),
     ("linwave_stress_10x8x6_s1", "linwave", (10, 8, 6), 1, 7),
+    # Fishbone-Moncrief torus, Kerr-Schild a=0.9, MKS: the reference's own
+    # initial data (loaded back so the counters start at zero), and the same
+    # with 5% of the zones replaced by extreme states
+    ("torus_24x16x8_s1", "torus", (24, 16, 8), 1, "load"),
+    ("torus_24x16x8_s3", "torus", (24, 16, 8), 3, "load"),
+    ("torus_stress_16x24x6_s1", "torus", (16, 24, 6), 1, 23),
 ]
 
 
@@ -59,6 +65,19 @@ def stress_state(p, seed):
     return p
 
 
+def sprinkle(p, seed):
+    """Replace 5% of the zones by extreme states (torus stress fixture)."""
+    rng = np.random.default_rng(seed)
+    p = p.copy()
+    sh = p.shape[:3]
+    m = rng.random(sh) < 0.05
+    k = int(m.sum())
+    p[m, 0] = 10 ** rng.uniform(-8, -1, k)
+    p[m, 1] = 10 ** rng.uniform(-9, -1, k)
+    p[m, 2:5] = rng.normal(0, 8, (k, 3))
+    return p
+
+
 def make(name, cfg, n, steps, seed):
     r0 = ht.run_ref(cfg, n, 1, dumps=[0], want_geom=True)
     s0 = r0["states"][0]
@@ -66,6 +85,12 @@ def make(name, cfg, n, steps, seed):
     if seed is None:
         load = None
         p0, t0, dt0 = s0["p"], s0["t"], s0["dt"]
+    elif seed == "load":
+        p0, t0, dt0 = s0["p"], s0["t"], s0["dt"]
+        load = dict(p=p0, t=t0, dt=dt0)
+    elif cfg == "torus":
+        p0, t0, dt0 = sprinkle(s0["p"], seed), s0["t"], s0["dt"]
+        load = dict(p=p0, t=t0, dt=dt0)
     else:
         p0 = stress_state(s0["p"], seed)
         t0, dt0 = s0["t"], 1e-4
@@ -80,8 +105,13 @@ def make(name, cfg, n, steps, seed):
         gam=geom["gam"], cour=geom["cour"], grid_length=geom["grid_length"], startx=geom["startx"],
         dx=geom["dx"], geom=geom["geom"], conn=geom["conn"],
         **{"sw_" + k: v for k, v in sw.items()})
-    # floors at every cell centre (the engine's builder is checked against these)
+    # floors at every cell centre (the engine's builder is checked against these),
+    # r along the line (i, N2S, N3S), r at FACE1 and the cooling tables per i
     out["cell_floors"] = geom["cell6"][..., :2]
+    out["r_line"] = geom["cell6"][:, ht.NG, ht.NG, 2]
+    out["rface"] = geom["rface"]
+    out["cool_omega"] = geom["cool_omega"]
+    out["cool_temp"] = geom["cool_temp"]
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(name, "nfailtot", s["nfailtot"].tolist())
 

@@ -28,7 +28,9 @@ CONFIG_SWITCHES = {
     "linwave_vl": dict(recon=4, flux=0, ct_para=1, bc=1, metric_dim=0, ee=1, cooling=0, rescale=0),
     "balsara1_noee": dict(recon=2, flux=1, ct_para=1, bc=0, metric_dim=0, ee=0, cooling=0, rescale=0),
     "linwave_noee": dict(recon=5, flux=1, ct_para=1, bc=1, metric_dim=0, ee=0, cooling=0, rescale=0),
+    "torus": dict(recon=5, flux=1, ct_para=1, bc=10, metric_dim=2, ee=1, cooling=1, rescale=1),
 }
+CONFIG_HOR = 0.1  # h_o_r of the torus build's cooling function
 
 
 def tot(n):
@@ -76,8 +78,11 @@ def read_geom(path, n):
     conn = np.frombuffer(b, np.float64, nconn * 64, o).reshape(nconn, 64).copy(); o += nconn * 64 * 8
     shp = (tot(n[0]), tot(n[1]), tot(n[2]))
     cell6 = np.frombuffer(b, np.float64, shp[0] * shp[1] * shp[2] * 6, o).reshape(shp + (6,)).copy()
+    o += shp[0] * shp[1] * shp[2] * 6 * 8
+    per_i = np.frombuffer(b, np.float64, shp[0] * 3, o).reshape(shp[0], 3).copy()
     return dict(gam=prm[0], cour=prm[1], grid_length=prm[2:6].copy(), startx=prm[6:10].copy(),
-                dx=prm[10:14].copy(), geom=geom, conn=conn, cell6=cell6)
+                dx=prm[10:14].copy(), geom=geom, conn=conn, cell6=cell6, rface=per_i[:, 0].copy(),
+                cool_omega=per_i[:, 1].copy(), cool_temp=per_i[:, 2].copy())
 
 
 def ref_exe(cfg):
@@ -101,6 +106,8 @@ def run_ref(cfg, n, steps, load=None, dumps=(), want_geom=False, timeout=600):
         env["HARM_PROBE_DUMP"] = ",".join(str(x) for x in dl)
         if want_geom:
             env["HARM_PROBE_GEOM"] = os.path.join(td, "geom.bin")
+            if CONFIG_SWITCHES[cfg]["cooling"]:
+                env["HARM_PROBE_HOR"] = repr(CONFIG_HOR)
         if load is not None:
             lp = os.path.join(td, "load.bin")
             write_state(lp, load["p"], load["t"], load["dt"])
@@ -144,6 +151,7 @@ def oracle_lib():
         lib.or_get_time.argtypes = [P, P, P, P]
         lib.or_step.argtypes = [P, ctypes.c_int]
         lib.or_face_flux.argtypes = [P, ctypes.c_int, P, P]
+        lib.or_set_cooling.argtypes = [P, P, P]
         lib.or_ntot.restype = ctypes.c_long
         lib.or_ntot.argtypes = [P]
         _olib = lib
@@ -174,6 +182,10 @@ class Oracle:
         self._keep = [np.ascontiguousarray(geomd["geom"]), np.ascontiguousarray(geomd["conn"]),
                       np.ascontiguousarray(geomd["cell6"]), geomd.get("rface")]
         self.h = self.lib.or_create(ctypes.byref(d), *(_ptr(x) for x in self._keep))
+        if sw["cooling"]:
+            om = np.ascontiguousarray(geomd["cool_omega"], np.float64)
+            te = np.ascontiguousarray(geomd["cool_temp"], np.float64)
+            self.lib.or_set_cooling(self.h, _ptr(om), _ptr(te))
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -50,7 +50,7 @@ def test_init_rejects_unsupported_switches():
     assert lib.hg_init(None, ctypes.byref(ctypes.c_void_p())) == -2
 
 
-@pytest.mark.parametrize("name", [n for n in fixtures.names() if "stress" not in n])
+@pytest.mark.parametrize("name", [n for n in fixtures.names() if "stress" not in n and not n.startswith("torus")])
 def test_minkowski_builder_matches_reference_tables(name):
     f = fixtures.load(name)
     d = hg.make_desc(f["n"], f["gam"], f["cour"], f["dx"], f["startx"], f["grid_length"])

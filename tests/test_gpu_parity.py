@@ -28,13 +28,24 @@ SW_TO_DESC = dict(recon="recon", flux="flux", ct_para="ct_para", bc="bc", metric
 
 
 def engine_for(n, sw, prm, p0, t0, dt0):
+    """Engine with the fixture's switches.  Minkowski runs take the host
+    builder's tables; curved-space runs the reference's own tables (what the
+    driver hands over through hg_set_geometry in a drop-in build)."""
     d = hg.make_desc(n, prm["gam"], prm["cour"], prm["dx"], prm["startx"], prm["grid_length"], t=t0,
                      recon=sw["recon"], flux=sw["flux"], ct_para=sw["ct_para"], bc=sw["bc"],
-                     metric_dim=sw["metric_dim"], use_ee=sw["ee"])
-    geom, cell6 = hg.minkowski_tables(d)
+                     metric_dim=sw["metric_dim"], use_ee=sw["ee"], cooling=sw["cooling"],
+                     rescale_r=sw["rescale"])
     e = hg.Engine(d)
-    e.set_geometry(geom)
-    e.set_cell_data(cell6)
+    if sw["metric_dim"] == 0:
+        geom, cell6 = hg.minkowski_tables(d)
+        e.set_geometry(geom)
+        e.set_cell_data(cell6)
+    else:
+        cell6 = fixtures.cell6_of(prm)
+        e.set_geometry(prm["geom"], prm["conn"])
+        e.set_cell_data(cell6, prm["rface"] if sw["rescale"] else None)
+    if sw["cooling"]:
+        e.set_cooling_tables(prm["cool_omega"], prm["cool_temp"])
     e.upload(p0)
     e.set_time(t0, dt0)
     return e, cell6
@@ -70,7 +81,20 @@ def assert_same(e, ref, n, check_nfail=True, rtol=0.0):
     assert e.fail_counts().tolist() == ref["nfailtot"].tolist()
     if check_nfail:
         if min(n) > 1:
-            assert np.array_equal(e.nfail(), ref["nfail"])
+            nf = e.nfail()
+            diff = nf.astype(np.int64) - ref["nfail"]
+            if ref.get("sw", {}).get("cooling"):
+                # The reference's first call of cooling_func_hr_disk leaves
+                # icurr at (N1TOT-1, N2S, N3S) (phys.c:683-690): the rest of
+                # that zone's bookings land on that ghost cell.  Counts may
+                # move between exactly that cell and one zone, nothing else.
+                cells = np.unique(np.argwhere(diff != 0)[:, 1:], axis=0)
+                assert len(cells) in (0, 2), cells.tolist()
+                assert diff.sum(axis=(1, 2, 3)).tolist() == [0] * hg.NFAIL
+                if len(cells):
+                    assert [n[0] + 5, 3, 3] in cells.tolist()
+            else:
+                assert not diff.any()
         else:
             nf = e.nfail()
             for s in range(hg.NFAIL):

@@ -11,10 +11,7 @@ import harmtest as ht
 
 
 def oracle_for(f):
-    shape = tuple(x + 2 * ht.NG for x in f["n"])
-    cell6 = np.zeros(shape + (6,))
-    cell6[..., :2] = f["cell_floors"]
-    return ht.Oracle(f["n"], f["sw"], fixtures.geomd(f, cell6))
+    return ht.Oracle(f["n"], f["sw"], fixtures.geomd(f))
 
 
 @pytest.mark.parametrize("name", fixtures.names())

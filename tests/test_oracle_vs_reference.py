@@ -9,7 +9,21 @@ import harmtest as ht
 
 CASES = [("balsara1", (200, 1, 1), 40, None), ("balsara1_lf", (90, 1, 1), 25, None),
          ("linwave", (9, 7, 5), 3, 3), ("linwave_vl", (6, 6, 6), 2, 9), ("balsara1", (48, 1, 1), 3, 21),
-         ("linwave", (1, 12, 10), 2, 4), ("linwave", (8, 1, 7), 2, 13)]
+         ("linwave", (1, 12, 10), 2, 4), ("linwave", (8, 1, 7), 2, 13), ("torus", (20, 12, 6), 4, "load"),
+         ("torus", (12, 20, 4), 2, 31)]
+
+
+def _sprinkle(p, seed):
+    return _mg().sprinkle(p, seed)
+
+
+def _mg():
+    import importlib.util, os
+    spec = importlib.util.spec_from_file_location(
+        "mg", os.path.join(os.path.dirname(__file__), "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg
 
 
 def _stress(p, seed):
@@ -29,6 +43,10 @@ def test_oracle_matches_live_reference(cfg, n, steps, seed):
     s0 = r0["states"][0]
     if seed is None:
         load, p0, t0, dt0 = None, s0["p"], s0["t"], s0["dt"]
+    elif seed == "load" or cfg == "torus":
+        p0 = s0["p"] if seed == "load" else _sprinkle(s0["p"], seed)
+        t0, dt0 = s0["t"], s0["dt"]
+        load = dict(p=p0, t=t0, dt=dt0)
     else:
         p0, t0, dt0 = _stress(s0["p"], seed), s0["t"], 1e-4
         load = dict(p=p0, t=t0, dt=dt0)
