@@ -44,7 +44,8 @@ class GridDesc(ctypes.Structure):
 EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", "hg_download_prims",
            "hg_upload_prims_tree", "hg_download_prims_tree", "hg_set_time", "hg_step", "hg_get_fail_counts",
            "hg_download_pflag", "hg_download_gamma", "hg_download_nfail", "hg_get_diag", "hg_last_step_ms",
-           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc", "hg_set_cooling_tables"]
+           "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc", "hg_set_cooling_tables",
+           "hg_build_geometry_ks_mks", "hg_fixup_bounds"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 _lib = None
@@ -80,6 +81,10 @@ def load_library(path=LIB_PATH):
     lib.hg_face_flux.argtypes = [P, ctypes.c_int32, P, P]
     lib.hg_set_cooling_tables.argtypes = [P, P, P]
     lib.hg_face_flux_noalloc.argtypes = [ctypes.POINTER(GridDesc), P, P, P, P, ctypes.c_int32, P]
+    D = ctypes.c_double
+    lib.hg_fixup_bounds.argtypes = [P]
+    lib.hg_build_geometry_ks_mks.argtypes = [ctypes.POINTER(GridDesc), D, D, D, D, ctypes.c_int32, D,
+                                             P, P, P, P, P, P]
     for fn in EXPORTS:
         if fn not in ("hg_destroy", "hg_strerror"):
             getattr(lib, fn).restype = I
@@ -128,6 +133,27 @@ def minkowski_tables(desc):
     _check(lib.hg_build_geometry_minkowski(ctypes.byref(desc), _ptr(geom), _ptr(cell6)),
            "hg_build_geometry_minkowski")
     return geom, cell6
+
+
+def ks_mks_tables(desc, a, R0=0.0, h_slope=0.35, th_cutout=1e-15 * np.pi, diag3_exponent=7, h_o_r=0.1):
+    """Geometry, connection, per-zone data, FACE1 radii and H/R cooling tables
+    of Kerr-Schild space-time in COORD_DIAGONAL3 modified Kerr-Schild
+    coordinates (host builder).  diag3_factor = 1 - 2 th_cutout/pi - h_slope,
+    as set_special_coord() sets it (init.torus.c:254-269).  Returns a dict with
+    geom (5*N1TOT*N2TOT, 42), conn (N1*N2, 64), cell6, rface, cool_omega,
+    cool_temp."""
+    lib = load_library()
+    n1, n2, n3 = desc.n1, desc.n2, desc.n3
+    shp = ref_shape((n1, n2, n3))
+    out = dict(geom=np.zeros((5 * shp[0] * shp[1], NGEOM)), conn=np.zeros((n1 * n2, 64)),
+               cell6=np.zeros(shp + (6,)), rface=np.zeros(shp[0]), cool_omega=np.zeros(shp[0]),
+               cool_temp=np.zeros(shp[0]))
+    diag3_factor = 1.0 - 2 * th_cutout / np.pi - h_slope
+    _check(lib.hg_build_geometry_ks_mks(ctypes.byref(desc), a, R0, h_slope, diag3_factor, diag3_exponent, h_o_r,
+                                        *[_ptr(out[k]) for k in ("geom", "conn", "cell6", "rface", "cool_omega",
+                                                                 "cool_temp")]),
+           "hg_build_geometry_ks_mks")
+    return out
 
 
 class Engine:
@@ -205,6 +231,11 @@ class Engine:
         v = np.empty((NFAIL,) + self.shape, np.int32)
         _check(self.lib.hg_download_nfail(self.h, _ptr(v)), "hg_download_nfail")
         return v
+
+    def fixup_bounds(self):
+        """Floors and gamma ceiling over the physical zones, then the boundary
+        zones, on the resident primitives (the setups' fixup(p); bounds(p,0))."""
+        _check(self.lib.hg_fixup_bounds(self.h), "hg_fixup_bounds")
 
     def face_flux(self, d):
         """(flux of direction d in the reference layout, max char speed)."""

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libharmgpu.so")
-SOURCES = ["hg_kernels.cu", "hg_api.cu"]
+SOURCES = ["hg_kernels.cu", "hg_api.cu", "hg_geometry.cu"]
 HEADERS = ["hg_internal.h", "hg_phys.cuh", "hg_fallback.cuh"]
 
 

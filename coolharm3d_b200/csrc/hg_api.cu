@@ -19,6 +19,7 @@
 namespace hg {
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R);
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d);
+void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 }  // namespace hg
 
 using hg::GridDev;
@@ -449,6 +450,17 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
   if (sc.err) return HG_ERR_DEVICE;
   if (t) *t = sc.t;
   if (dt) *dt = sc.dt;
+  return HG_OK;
+}
+
+extern "C" int hg_fixup_bounds(hg_handle *h)
+{
+  if (!h) return HG_ERR_BADARG;
+  if (!h->have_geom || !h->have_cells || !h->have_prims) return HG_ERR_STATE;
+  HG_CK(cudaSetDevice(h->d.device));
+  hg::launch_fixup_bounds(h->G, h->L, h->stream);
+  HG_CK(cudaGetLastError());
+  HG_CK(cudaStreamSynchronize(h->stream));
   return HG_OK;
 }
 

@@ -913,6 +913,48 @@ __global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict_
 }
 
 // ---------------------------------------------------------------------------
+// fixup(), fixup.c:8-33 with fixup1zone (fixup.c:45-75): over the physical
+// zones, gamma_calc (FAIL_GAMMA_CALC, gamma = 1 on failure), the rho/u floors
+// (FAIL_FLOOR) and the gamma ceiling fixup_gamma (fixup.c:148-158,
+// FAIL_GAMMA_MAX); all with state 0, so no zone is flagged.  This is the
+// init-time pass the setups run before and after the magnetic field is set
+// (init.torus.c:205-215).
+__global__ void __launch_bounds__(HG_BLK) k_fixup_cells(GridDev G)
+{
+  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
+  const long total = (long)N0 * N1 * N2;
+  const long S = G.S;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = HG_NGH + (int)(t % N0);
+    const int j = HG_NGH + (int)((t / N0) % N1);
+    const int k = HG_NGH + (int)(t / ((long)N0 * N1));
+    const long o = off3(G, i, j, k);
+    Geom g;
+    if (G.mdim != 0) load_geom(G, 3, i, j, g);
+    else g = G.g0;
+    double pv[HG_NPR];
+    for (int l = 0; l < HG_NPR; l++) pv[l] = G.p[l * S + o];
+    double gamma;
+    if (gamma_calc(pv, g, &gamma)) {
+      book(G, NF_GAMMA_CALC, i, j, k);
+      gamma = 1.;
+    }
+    bool fl = false;
+    if (pv[RHO] < G.floors[o]) { pv[RHO] = G.floors[o]; fl = true; }
+    if (pv[UU] < G.floors[S + o]) { pv[UU] = G.floors[S + o]; fl = true; }
+    if (fl) book(G, NF_FLOOR, i, j, k);
+    if (check_gamma(gamma)) {
+      const double f = sqrt((HG_GAMMAMAX - 1.) * (HG_GAMMAMAX + 1.) / ((gamma - 1.) * (gamma + 1.)));
+      pv[U1] *= f;
+      pv[U2] *= f;
+      pv[U3] *= f;
+      book(G, NF_GAMMA_MAX, i, j, k);
+    }
+    for (int l = 0; l < HG_NPR; l++) G.p[l * S + o] = pv[l];
+  }
+}
+
+// ---------------------------------------------------------------------------
 __global__ void k_begin(DevScalars *sc)
 {
   sc->maxs[0] = sc->maxs[1] = sc->maxs[2] = sc->maxs[3] = 0ull;
@@ -1047,6 +1089,13 @@ void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int 
 {
   k_reset_max<<<1, 1, 0, s>>>(G.sc, d + 1);
   launch_flux_dir(G, L, s, G.p, d, nullptr);
+}
+
+void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
+{
+  k_begin<<<1, 1, 0, s>>>(G.sc);
+  k_fixup_cells<<<L.grid_upd, HG_BLK, 0, s>>>(G);
+  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0);
 }
 
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R)

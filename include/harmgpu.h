@@ -151,6 +151,13 @@ int hg_face_flux_noalloc(const hg_grid_desc *desc, const double *geom, const dou
  * characteristic speeds that set dx[0] (step_ch.c:716-724). */
 int hg_get_diag(hg_handle *h, double *m_tot, double max_char_speed[3]);
 
+/* fixup(p); bounds(p,0); of the setups' init_data() (init.torus.c:205-215):
+ * on the resident primitives, the rho/u floors and the gamma ceiling of
+ * fixup1zone() over the physical zones (fixup.c:8-75; failures counted with
+ * state 0, no zone flagged), then the boundary zones.  Setups call it between
+ * uploading initial data and computing fields that read ghost zones. */
+int hg_fixup_bounds(hg_handle *h);
+
 /* Device time of the last hg_step call in milliseconds (CUDA events). */
 int hg_last_step_ms(hg_handle *h, double *ms);
 
@@ -173,6 +180,24 @@ const char *hg_strerror(int code);
  * cell6 = N1TOT*N2TOT*N3TOT*6 with the r-dependent floors RHOMIN r^-1.5,
  * UUMIN r^-2.5 (options.h:233-240). */
 int hg_build_geometry_minkowski(const hg_grid_desc *desc, double *geom, double *cell6);
+
+/* Kerr-Schild space-time (M = 1, spin a) in modified Kerr-Schild coordinates
+ * COORD_DIAGONAL3 (coord.c:270-276, 3754-3800; metric.c:1168-1258), METRIC_DIM 2:
+ *   r = R0 + exp(x1),  th = pi/2 (1 + h_slope f + diag3_factor f^diag3_exponent),
+ *   f = 2 seesaw(x2, 0, 1) - 1,  phi = x3.
+ * Fills geom (5 * N1TOT * N2TOT structs, GEOM_ID order), conn (N1 * N2 * 64
+ * doubles, Gamma^a_bc at zone centres), cell6 (N1TOT*N2TOT*N3TOT*6: floors
+ * RHOMIN r^-1.5, UUMIN r^-2.5, r, r, th, phi), rface (N1TOT: r at FACE1) and,
+ * when both are non-NULL, the H/R cooling tables cool_omega / cool_temp
+ * (N1TOT: omega_circular_equatorial() and target_temperature() of
+ * phys.c:805-905 for h_o_r, with the ISCO radius the torus setup computes).
+ * The connection is derived from the metric by complex-step differentiation,
+ * so the tables agree with the reference's to rounding (relative 1e-12), not
+ * bit for bit.  HG_ERR_BADARG for |a| >= 1 or diag3_exponent < 3. */
+int hg_build_geometry_ks_mks(const hg_grid_desc *desc, double a, double R0, double h_slope,
+                             double diag3_factor, int32_t diag3_exponent, double h_o_r,
+                             double *geom, double *conn, double *cell6, double *rface,
+                             double *cool_omega, double *cool_temp);
 
 #ifdef __cplusplus
 }

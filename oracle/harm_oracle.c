@@ -1818,6 +1818,27 @@ void or_face_flux(or_ctx *c, int d, double *flux, double *mcs)
   *mcs = c->max_char_speed[d + 1];
 }
 
+/* init_data()'s fixup(p); bounds(p,0); (init.torus.c:205-215): fixup(),
+ * fixup.c:8-33, with fixup1zone(), fixup.c:45-75 (floors, gamma ceiling) */
+void or_fixup_bounds(or_ctx *c)
+{
+  int i, j, k;
+  for (i = NG; i < c->N1 + NG; i++)
+    for (j = NG; j < c->N2 + NG; j++)
+      for (k = NG; k < c->N3 + NG; k++) {
+        const geom_t *g = G(c, i, j, k, 3); /* CENT */
+        double *pv = &c->p[IX(c, i, j, k) * NP];
+        double gamma;
+        if (gamma_calc(pv, g, &gamma)) {
+          fail(c, F_GAMMA_CALC, 0);
+          gamma = 1.;
+        }
+        fixup_floor(c, pv, IX(c, i, j, k));
+        if (check_gamma(gamma)) fixup_gamma(c, pv, &gamma);
+      }
+  bounds(c, c->p);
+}
+
 void or_step(or_ctx *c, int nsteps)
 {
   for (int s = 0; s < nsteps; s++) step_ch(c);

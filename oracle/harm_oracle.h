@@ -66,6 +66,8 @@ void or_get_nfail(const or_ctx *c, int32_t *nfail);      /* [OR_NFAIL][NTOT] */
 void or_get_nfailtot(const or_ctx *c, uint64_t *nfailtot);
 void or_get_time(const or_ctx *c, double *t, double *dt, double *m_tot);
 void or_step(or_ctx *c, int nsteps);
+/* fixup(p); bounds(p,0); as the setups' init_data() calls them. */
+void or_fixup_bounds(or_ctx *c);
 /* reconstruct_fast + numerical_flux of the current primitives: the fluxes of
  * direction d (before flux_ct) in the reference layout, 0 on faces not
  * computed, and max_char_speed[d+1]. */

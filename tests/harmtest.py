@@ -150,6 +150,7 @@ def oracle_lib():
             getattr(lib, fn).argtypes = [P, P]
         lib.or_get_time.argtypes = [P, P, P, P]
         lib.or_step.argtypes = [P, ctypes.c_int]
+        lib.or_fixup_bounds.argtypes = [P]
         lib.or_face_flux.argtypes = [P, ctypes.c_int, P, P]
         lib.or_set_cooling.argtypes = [P, P, P]
         lib.or_ntot.restype = ctypes.c_long
@@ -198,6 +199,18 @@ class Oracle:
 
     def step(self, n=1):
         self.lib.or_step(self.h, n)
+
+    # the Engine methods a setup drives (upload / fixup_bounds / download)
+    def upload(self, p):
+        self.set_state(p, 0.0, 0.0)
+
+    def fixup_bounds(self):
+        self.lib.or_fixup_bounds(self.h)
+
+    def download(self):
+        p = np.empty(self.shape + (NP,))
+        self.lib.or_get_prims(self.h, _ptr(p))
+        return p
 
     def face_flux(self, d):
         f = np.empty(self.shape + (NP,))
