@@ -7,6 +7,13 @@ A step is one full RK2 step_ch() of the grid (predictor + corrector with
 boundaries, fixups and the CFL reduction).  Rank 0 prints one JSON line.
 
 Workloads (synthetic data of the configuration's shape; no dataset involved):
+  torus192    (default) magnetised Fishbone-Moncrief torus around a Kerr
+              black hole, a = 0.9, modified Kerr-Schild coordinates,
+              192x192x128 zones (r from inside the horizon to 120 M, full
+              2 pi in phi), r_in = 6 M, r_pmax = 12 M, Gamma = 5/3, one
+              poloidal loop scaled to beta 100, seeded +-2% u perturbation,
+              H/R = 0.1 cooling; PPM_MC + HLLE + para flux-CT, entropy fix,
+              RESCALE_R, spherical outflow-3 boundaries; FP64.
   linwave256  3D periodic Minkowski linear wave, 256^3 zones, Gamma=4/3,
               rho=1, p=1, B=(1,1.5,0), plane-wave perturbation of amplitude
               1e-6 along the grid diagonal; PPM_MC + HLLE + para flux-CT, FP64.
@@ -17,9 +24,10 @@ ranks, value = total zone-updates of all ranks / that time ("weak").
 
 The reference arm (--impl reference) times the reference's own CPU build
 (oracle/_ref/<config>/harm3d, made from the reference sources by
-oracle/build_ref.py) on the host cores: one process per core, each the
-64^3 block one rank of a 4x4x4 decomposition of the 256^3 grid would own,
-run without MPI (no halo exchange, so an upper bound on the MPI build).
+oracle/build_ref.py) on the host cores: one process per core, each running
+the same problem on the block one rank of a 4x4x4 decomposition would own
+(48x48x32 of the torus, 64^3 of the linear wave), without MPI (no halo
+exchange, so an upper bound on the MPI build's rate).
 """
 import argparse
 import json
@@ -46,16 +54,21 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="linwave256")
+    ap.add_argument("--workload", default="torus192")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
 WORKLOADS = {
-    "linwave256": dict(n=(256, 256, 256), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
+    "torus192": dict(kind="torus", n=(192, 192, 128), ref_cfg="torus", ref_block=(48, 48, 32),
+                     label="Fishbone-Moncrief torus, Kerr-Schild a=0.9, MKS 192x192x128, r_in 6, r_pmax 12, "
+                           "Gamma 5/3, beta 100 loop, H/R 0.1 cooling, PPM_MC+HLLE+para flux-CT, entropy fix, FP64"),
+    "torus96": dict(kind="torus", n=(96, 96, 64), ref_cfg="torus", ref_block=(24, 24, 16),
+                    label="Fishbone-Moncrief torus as torus192 on 96x96x64 zones"),
+    "linwave256": dict(kind="linwave", n=(256, 256, 256), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
                        ref_block=(64, 64, 64),
                        label="3D periodic Minkowski linear wave 256^3, PPM_MC+HLLE+para flux-CT, FP64"),
-    "linwave128": dict(n=(128, 128, 128), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
+    "linwave128": dict(kind="linwave", n=(128, 128, 128), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
                        ref_block=(32, 32, 32),
                        label="3D periodic Minkowski linear wave 128^3, PPM_MC+HLLE+para flux-CT, FP64"),
 }
@@ -163,9 +176,21 @@ def algorithmic_bytes(kind, n):
     return None
 
 
-def run_ours(args, wl, rank, world, device):
+def setup(wl, device):
+    """Engine holding the workload's initial state, and that state on the host."""
     import coolharm3d_b200 as hg
     n = wl["n"]
+    if wl["kind"] == "torus":
+        from coolharm3d_b200 import torus
+        desc = torus.torus_desc(n, device=device)
+        t = torus.torus_tables(desc)
+        e = hg.Engine(desc)
+        e.set_geometry(t["geom"], t["conn"])
+        e.set_cell_data(t["cell6"], t["rface"])
+        e.set_cooling_tables(t["cool_omega"], t["cool_temp"])
+        p0 = torus.set_torus(e, desc, t, seed=2024)
+        e.set_time(desc.t, desc.dx[0])
+        return e, p0
     dx = [1e-5] + [1.0 / x for x in n]
     startx = [0.0] + [-3 * d for d in dx[1:]]
     desc = hg.make_desc(n, wl["gam"], wl["cour"], dx, startx, [1e9, 1, 1, 1], recon=wl["recon"], flux=wl["flux"],
@@ -176,6 +201,13 @@ def run_ours(args, wl, rank, world, device):
     e.set_geometry(geom)
     e.set_cell_data(cell6)
     e.upload(p0)
+    return e, p0
+
+
+def run_ours(args, wl, rank, world, device):
+    import coolharm3d_b200 as hg
+    n = wl["n"]
+    e, p0 = setup(wl, device)
     zones = n[0] * n[1] * n[2]
     barrier, sync = lambda: None, lambda: None
     try:
@@ -207,6 +239,7 @@ def run_ours(args, wl, rank, world, device):
     host_p = np.ascontiguousarray(p0)
     t0 = time.perf_counter()
     e.upload(host_p)
+    e.set_time(e.desc.t, e.desc.dx[0])
     for _ in range(args.steps):
         e.step(1)
         e.fail_counts()
@@ -230,7 +263,8 @@ def run_ours(args, wl, rank, world, device):
                vs_baseline=None, dtype="f64", data="synthetic",
                config={"workload": args.workload, "description": wl["label"], "grid": list(n),
                        "zones": zones, "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (state arrays 1.1 GB each)",
+                       "l2": "inputs larger than L2 (state arrays of %.2f GB each)" % (
+                           8 * 8 * np.prod(hg.ref_shape(n)) / 1e9),
                        "e2e": "upload from host once + K x (hg_step(1) + nfailtot readback) + download once"})
     # roofline of the dominant kernel class (live CUDA events on the engine stream)
     dom = max(("flux", "update", "emf"), key=lambda c: kt[c][0])
