@@ -10,7 +10,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "harmgpu.h"
@@ -20,9 +22,17 @@ namespace hg {
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R);
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d);
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
+void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
+                          double *out);
+void launch_planes_to_ref(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *in, int NT0, int NT1,
+                          int NT2, double *ref);
 }  // namespace hg
 
 using hg::GridDev;
+
+#define HG_XCH_THREADS 8              // host threads of one transfer
+#define HG_XCH (2 * HG_XCH_THREADS)   // pinned staging slots, two per thread
+#define HG_XCH_BYTES (4L << 20)       // bytes per transfer chunk (a multiple of 64)
 
 struct hg_handle {
   hg_grid_desc d;
@@ -33,7 +43,9 @@ struct hg_handle {
   float last_ms = 0.f;
   bool have_geom = false, have_cells = false, have_prims = false, have_cool = false;
   std::vector<void *> allocs;
-  double *h_stage = nullptr;  // pinned staging buffer, 8 planes
+  double *h_stage = nullptr;  // pinned transfer chunks (HG_XCH x HG_XCH_BYTES)
+  cudaEvent_t xev[HG_XCH] = {};  // DMA completion of each transfer chunk
+  double *d_ref = nullptr;    // device buffer in the reference layout, when F[0] is too small
   long ntot_ref = 0;          // N1TOT*N2TOT*N3TOT of the reference layout
   int NT[3] = {0, 0, 0};      // reference extents
   // per-kernel-class timing (hg_profile)
@@ -192,7 +204,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     h->L.grid_fix = grid_for(G.capacity, 4);
     h->L.grid_bnd = grid_for(faces - G.capacity, 8);
     ALLOC(G.blk, sizeof(double) * h->L.grid_upd);
-    if (cudaMallocHost((void **)&h->h_stage, S8 * HG_NPR) != cudaSuccess) {
+    if (cudaMallocHost((void **)&h->h_stage, (size_t)HG_XCH * HG_XCH_BYTES) != cudaSuccess) {
       cudaGetLastError();
       rc = HG_ERR_NOMEM;
       goto fail;
@@ -202,6 +214,11 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
       rc = HG_ERR_CUDA;
       goto fail;
     }
+    for (int x = 0; x < HG_XCH; x++)
+      if (cudaEventCreateWithFlags(&h->xev[x], cudaEventDisableTiming) != cudaSuccess) {
+        rc = HG_ERR_CUDA;
+        goto fail;
+      }
     hg::DevScalars sc0;
     memset(&sc0, 0, sizeof(sc0));
     sc0.t = desc->t;
@@ -227,6 +244,8 @@ extern "C" void hg_destroy(hg_handle *h)
   for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_stage) cudaFreeHost(h->h_stage);
+  for (int x = 0; x < HG_XCH; x++)
+    if (h->xev[x]) cudaEventDestroy(h->xev[x]);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -332,20 +351,79 @@ extern "C" int hg_set_cooling_tables(hg_handle *h, const double *omega, const do
   return HG_OK;
 }
 
-template <class GET>
-static int upload_impl(hg_handle *h, GET get)
+// Host <-> device transfer of the primitives in the reference layout.  The
+// reference-ordered array (N1TOT*N2TOT*N3TOT zones of 8 doubles) moves as a
+// byte stream of HG_XCH_BYTES chunks through pinned staging slots: up to
+// HG_XCH_THREADS host threads each copy their share of chunks between the
+// caller's memory and two slots of their own, so host copies overlap one
+// another and the DMA of the other chunks.  On the device the stream lands
+// in a buffer in the same layout, and a kernel converts it to or from the
+// resident planes.  That buffer is F[0] (dead between steps) when the
+// reference layout is no larger than the planes, else a buffer of its own.
+static double *ref_buffer(hg_handle *h)
+{
+  if (h->ntot_ref <= h->G.S) return h->G.F[0];
+  if (!h->d_ref) {
+    void *q = nullptr;
+    if (dev_alloc(h, &q, sizeof(double) * HG_NPR * h->ntot_ref) != HG_OK) return nullptr;
+    h->d_ref = (double *)q;
+  }
+  return h->d_ref;
+}
+
+// Runs work(w, nw) on nw = min(HG_XCH_THREADS, chunks) threads (the calling
+// thread is worker 0); returns the first non-success status.
+template <class W>
+static cudaError_t run_workers(long nch, W work)
+{
+  const int nw = (int)std::max<long>(1, std::min<long>(nch, HG_XCH_THREADS));
+  std::vector<cudaError_t> st(nw, cudaSuccess);
+  std::vector<std::thread> th;
+  int started = 1;
+  for (int w = 1; w < nw; w++, started++) {
+    try {
+      th.emplace_back([&st, &work, w, nw] { st[w] = work(w, nw); });
+    } catch (...) {
+      break;
+    }
+  }
+  // worker 0 takes its own chunks and those of any worker not started
+  st[0] = work(0, nw);
+  for (int w = started; w < nw; w++) st[w] = work(w, nw);
+  for (auto &t : th) t.join();
+  for (cudaError_t e : st)
+    if (e != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+// FILL(dst, first zone, zones) writes that many zones of the reference order
+template <class FILL>
+static int upload_impl(hg_handle *h, FILL fill)
 {
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
-  double *st = h->h_stage;
-  for (int k = 0; k < G.T[2]; k++)
-    for (int j = 0; j < G.T[1]; j++)
-      for (int i = 0; i < G.T[0]; i++) {
-        const double *src = get(ref_of(G, 0, i), ref_of(G, 1, j), ref_of(G, 2, k));
-        const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
-        for (int l = 0; l < HG_NPR; l++) st[l * G.S + o] = src[l];
-      }
-  HG_CK(cudaMemcpyAsync(G.p, st, sizeof(double) * HG_NPR * G.S, cudaMemcpyHostToDevice, h->stream));
+  double *dref = ref_buffer(h);
+  if (!dref) return HG_ERR_NOMEM;
+  const long zc = HG_XCH_BYTES / (sizeof(double) * HG_NPR);  // zones per chunk
+  const long nch = (h->ntot_ref + zc - 1) / zc;
+  const int dev = h->d.device;
+  HG_CK(run_workers(nch, [&](int w, int nw) -> cudaError_t {
+    cudaError_t e = cudaSetDevice(dev);
+    long n = 0;
+    for (long c = w; c < nch && e == cudaSuccess; c += nw, n++) {
+      const int slot = 2 * w + (int)(n & 1);
+      const long z0 = c * zc, nz = std::min(zc, h->ntot_ref - z0);
+      double *hb = h->h_stage + (long)slot * zc * HG_NPR;
+      if (n >= 2) e = cudaEventSynchronize(h->xev[slot]);
+      if (e != cudaSuccess) break;
+      fill(hb, z0, nz);
+      e = cudaMemcpyAsync(dref + z0 * HG_NPR, hb, sizeof(double) * HG_NPR * nz, cudaMemcpyHostToDevice, h->stream);
+      if (e == cudaSuccess) e = cudaEventRecord(h->xev[slot], h->stream);
+    }
+    return e;
+  }));
+  hg::launch_ref_to_planes(G, h->L, h->stream, dref, h->NT[1], h->NT[2], G.p);
+  HG_CK(cudaGetLastError());
   HG_CK(cudaMemsetAsync(G.nfail, 0, sizeof(unsigned int) * HG_NF * G.S, h->stream));
   HG_CK(cudaMemsetAsync(G.pflag, 0, sizeof(int) * G.S, h->stream));
   HG_CK(cudaMemsetAsync(sc_field(G, offsetof(hg::DevScalars, nfailtot)), 0, sizeof(unsigned long long) * 16, h->stream));
@@ -354,48 +432,94 @@ static int upload_impl(hg_handle *h, GET get)
   return HG_OK;
 }
 
-template <class PUT>
-static int download_impl(hg_handle *h, PUT put)
+// DRAIN(src, first zone, zones) reads that many zones of the reference order
+template <class DRAIN>
+static int download_impl(hg_handle *h, DRAIN drain)
 {
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
-  double *st = h->h_stage;
-  HG_CK(cudaMemcpyAsync(st, G.p, sizeof(double) * HG_NPR * G.S, cudaMemcpyDeviceToHost, h->stream));
-  HG_CK(cudaStreamSynchronize(h->stream));
-  for (int i = 0; i < h->NT[0]; i++)
-    for (int j = 0; j < h->NT[1]; j++)
-      for (int k = 0; k < h->NT[2]; k++) {
-        double *dst = put(i, j, k);
-        const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
-        for (int l = 0; l < HG_NPR; l++) dst[l] = st[l * G.S + o];
+  double *dref = ref_buffer(h);
+  if (!dref) return HG_ERR_NOMEM;
+  hg::launch_planes_to_ref(G, h->L, h->stream, G.p, h->NT[0], h->NT[1], h->NT[2], dref);
+  HG_CK(cudaGetLastError());
+  const long zc = HG_XCH_BYTES / (sizeof(double) * HG_NPR);
+  const long nch = (h->ntot_ref + zc - 1) / zc;
+  const int dev = h->d.device;
+  HG_CK(run_workers(nch, [&](int w, int nw) -> cudaError_t {
+    cudaError_t e = cudaSetDevice(dev);
+    // two chunks in flight per worker: issue c, then drain c - nw
+    long prev = -1;
+    int n = 0;
+    for (long c = w; e == cudaSuccess; c += nw, n++) {
+      if (c < nch) {
+        const int slot = 2 * w + (n & 1);
+        const long z0 = c * zc, nz = std::min(zc, h->ntot_ref - z0);
+        e = cudaMemcpyAsync(h->h_stage + (long)slot * zc * HG_NPR, dref + z0 * HG_NPR, sizeof(double) * HG_NPR * nz,
+                            cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(h->xev[slot], h->stream);
+        if (e != cudaSuccess) break;
       }
+      if (prev >= 0) {
+        const int slot = 2 * w + ((n - 1) & 1);
+        const long z0 = prev * zc, nz = std::min(zc, h->ntot_ref - z0);
+        e = cudaEventSynchronize(h->xev[slot]);
+        if (e != cudaSuccess) break;
+        drain(h->h_stage + (long)slot * zc * HG_NPR, z0, nz);
+      }
+      if (c >= nch) break;
+      prev = c;
+    }
+    return e;
+  }));
   return HG_OK;
 }
 
 extern "C" int hg_upload_prims(hg_handle *h, const double *p)
 {
   if (!h || !p) return HG_ERR_BADARG;
-  const int N2T = h->NT[1], N3T = h->NT[2];
-  return upload_impl(h, [&](int i, int j, int k) { return p + (((long)i * N2T + j) * N3T + k) * HG_NPR; });
+  return upload_impl(h, [&](double *dst, long z0, long nz) {
+    memcpy(dst, p + z0 * HG_NPR, sizeof(double) * HG_NPR * nz);
+  });
 }
 
 extern "C" int hg_download_prims(hg_handle *h, double *p)
 {
   if (!h || !p) return HG_ERR_BADARG;
-  const int N2T = h->NT[1], N3T = h->NT[2];
-  return download_impl(h, [&](int i, int j, int k) { return p + (((long)i * N2T + j) * N3T + k) * HG_NPR; });
+  return download_impl(h, [&](const double *src, long z0, long nz) {
+    memcpy(p + z0 * HG_NPR, src, sizeof(double) * HG_NPR * nz);
+  });
+}
+
+// zone z of the reference order -> (i, j, k)
+static inline void ref_ijk(const hg_handle *h, long z, int &i, int &j, int &k)
+{
+  k = (int)(z % h->NT[2]);
+  j = (int)((z / h->NT[2]) % h->NT[1]);
+  i = (int)(z / ((long)h->NT[2] * h->NT[1]));
 }
 
 extern "C" int hg_upload_prims_tree(hg_handle *h, double ****p)
 {
   if (!h || !p) return HG_ERR_BADARG;
-  return upload_impl(h, [&](int i, int j, int k) { return (const double *)p[i][j][k]; });
+  return upload_impl(h, [&](double *dst, long z0, long nz) {
+    for (long z = 0; z < nz; z++) {
+      int i, j, k;
+      ref_ijk(h, z0 + z, i, j, k);
+      memcpy(dst + z * HG_NPR, p[i][j][k], sizeof(double) * HG_NPR);
+    }
+  });
 }
 
 extern "C" int hg_download_prims_tree(hg_handle *h, double ****p)
 {
   if (!h || !p) return HG_ERR_BADARG;
-  return download_impl(h, [&](int i, int j, int k) { return p[i][j][k]; });
+  return download_impl(h, [&](const double *src, long z0, long nz) {
+    for (long z = 0; z < nz; z++) {
+      int i, j, k;
+      ref_ijk(h, z0 + z, i, j, k);
+      memcpy(p[i][j][k], src + z * HG_NPR, sizeof(double) * HG_NPR);
+    }
+  });
 }
 
 extern "C" int hg_set_time(hg_handle *h, double t, double dt)

@@ -29,6 +29,9 @@
 namespace hg {
 
 #define HG_BLK 128
+#ifndef HG_UPD_MINB
+#define HG_UPD_MINB 1
+#endif
 #ifndef HG_FLUX_MINB
 #define HG_FLUX_MINB 4
 #endif
@@ -397,7 +400,7 @@ __device__ __forceinline__ void update_zone(const GridDev &G, int i, int j, int 
 
 // k_update: every physical zone.  sub = 0 predictor (p_f = ph), 1 corrector (p_f = p).
 template <bool RS, int MDIM>
-__global__ void __launch_bounds__(HG_BLK) k_update(const __grid_constant__ GridDev G, int sub, double dtfac,
+__global__ void __launch_bounds__(HG_BLK, HG_UPD_MINB) k_update(const __grid_constant__ GridDev G, int sub, double dtfac,
                                                    const double *__restrict__ p_h, double *__restrict__ p_f)
 {
   const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
@@ -1083,6 +1086,57 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
 }
 
 __global__ void k_reset_max(DevScalars *sc, int dim) { sc->maxs[dim] = 0ull; }
+
+// ---------------------------------------------------------------------------
+// Layout conversion between the reference's p[i][j][k][l] (NP innermost,
+// every direction N+6 long) and the resident planes.  One thread per stored
+// zone in the reference's order (k fastest), so the reference-side array is
+// read/written in contiguous 64-byte runs.  A degenerate direction reads its
+// one stored copy from the ghost-free reference index NG, and writes every
+// reference copy of that direction.
+__global__ void __launch_bounds__(HG_BLK) k_ref_to_planes(GridDev G, const double *__restrict__ ref, int NT1, int NT2,
+                                                          double *__restrict__ out)
+{
+  const long total = G.S;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % G.T[2]);
+    const int j = (int)((t / G.T[2]) % G.T[1]);
+    const int i = (int)(t / ((long)G.T[2] * G.T[1]));
+    const int ri = G.deg[0] ? HG_NGH : i, rj = G.deg[1] ? HG_NGH : j, rk = G.deg[2] ? HG_NGH : k;
+    const double *src = ref + (((long)ri * NT1 + rj) * NT2 + rk) * HG_NPR;
+    const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) out[l * G.S + o] = src[l];
+  }
+}
+
+__global__ void __launch_bounds__(HG_BLK) k_planes_to_ref(GridDev G, const double *__restrict__ in, int NT0, int NT1,
+                                                          int NT2, double *__restrict__ ref)
+{
+  const long total = (long)NT0 * NT1 * NT2;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int rk = (int)(t % NT2);
+    const int rj = (int)((t / NT2) % NT1);
+    const int ri = (int)(t / ((long)NT2 * NT1));
+    const int i = G.deg[0] ? 0 : ri, j = G.deg[1] ? 0 : rj, k = G.deg[2] ? 0 : rk;
+    const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+    double *dst = ref + t * HG_NPR;
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) dst[l] = in[l * G.S + o];
+  }
+}
+
+void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
+                          double *out)
+{
+  k_ref_to_planes<<<L.grid_flux, HG_BLK, 0, s>>>(G, ref, NT1, NT2, out);
+}
+
+void launch_planes_to_ref(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *in, int NT0, int NT1,
+                          int NT2, double *ref)
+{
+  k_planes_to_ref<<<L.grid_flux, HG_BLK, 0, s>>>(G, in, NT0, NT1, NT2, ref);
+}
 
 // Fluxes of direction d from the resident primitives G.p (hg_face_flux).
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d)
