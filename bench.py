@@ -272,17 +272,22 @@ def run_ours(args, wl, rank, world, device):
     alg = algorithmic_bytes(dom, n)
     peak, src = peak_hbm()
     ach = alg / (avg_ms * 1e-3) / 1e9
-    traffic = None
+    traffic, fp64 = None, None
     tf = os.path.join(HERE, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(args.workload, {}).get(dom)
+            rec = json.load(open(tf)).get(args.workload, {})
+            traffic = rec.get(dom)
+            fp64 = rec.get("fp64_pipe_active", {}).get(dom)
         except (OSError, ValueError):
             traffic = None
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "peak_source": src,
                        "unit": "GB/s", "frac": ach / peak, "traffic": traffic,
                        "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": alg,
-                       "kernel_share": {c: kt[c][0] / max(sum(v[0] for v in kt.values()), 1e-30) for c in kt}}
+                       "kernel_share": {c: kt[c][0] / max(sum(v[0] for v in kt.values()), 1e-30) for c in kt},
+                       "fp64_pipe_active_ncu": fp64,
+                       "note": "the step is FP64-issue bound; fp64_pipe_active_ncu is the FP64 pipe's active "
+                               "fraction for this kernel from the committed ncu capture"}
     out["e2e"] = {"value": e2e_val, "unit": "zone-updates/s",
                   "h2d_bytes_per_step": float(state_bytes) / args.steps,
                   "d2h_bytes_per_step": float(state_bytes) / args.steps + 16 + 120}
