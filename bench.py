@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="torus192")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed-steps", type=int, default=2000,
+                    help="steps of the mixed-precision accuracy comparison (0: skip the mixed form)")
     return ap.parse_args()
 
 
@@ -176,27 +178,33 @@ def algorithmic_bytes(kind, n):
     return None
 
 
-def setup(wl, device):
-    """Engine holding the workload's initial state, and that state on the host."""
+def setup(wl, device, precision=0, p_init=None):
+    """Engine holding the workload's initial state, and that state on the host.
+    precision 1 builds the mixed-precision engine; p_init, if given, is
+    uploaded instead of a freshly built initial state."""
     import coolharm3d_b200 as hg
     n = wl["n"]
     if wl["kind"] == "torus":
         from coolharm3d_b200 import torus
-        desc = torus.torus_desc(n, device=device)
+        desc = torus.torus_desc(n, device=device, precision=precision)
         t = torus.torus_tables(desc)
         e = hg.Engine(desc)
         e.set_geometry(t["geom"], t["conn"])
         e.set_cell_data(t["cell6"], t["rface"])
         e.set_cooling_tables(t["cool_omega"], t["cool_temp"])
-        p0 = torus.set_torus(e, desc, t, seed=2024)
+        if p_init is None:
+            p0 = torus.set_torus(e, desc, t, seed=2024)
+        else:
+            p0 = p_init
+            e.upload(p0)
         e.set_time(desc.t, desc.dx[0])
         return e, p0
     dx = [1e-5] + [1.0 / x for x in n]
     startx = [0.0] + [-3 * d for d in dx[1:]]
     desc = hg.make_desc(n, wl["gam"], wl["cour"], dx, startx, [1e9, 1, 1, 1], recon=wl["recon"], flux=wl["flux"],
-                        bc=wl["bc"], device=device)
+                        bc=wl["bc"], device=device, precision=precision)
     geom, cell6 = hg.minkowski_tables(desc)
-    p0 = linwave_state(n, wl["gam"])
+    p0 = linwave_state(n, wl["gam"]) if p_init is None else p_init
     e = hg.Engine(desc)
     e.set_geometry(geom)
     e.set_cell_data(cell6)
@@ -295,7 +303,56 @@ def run_ours(args, wl, rank, world, device):
     out["gpu_launches"] = int(sum(v[1] for v in kt.values()))
     if clocks:
         out["clocks"] = clocks
+    if rank == 0 and args.mixed_steps > 0:
+        out["mixed"] = mixed_form(args, wl, device, e, p0, ms / args.steps)
+    e.close()
     return out
+
+
+VARS = ["rho", "u", "U1", "U2", "U3", "B1", "B2", "B3"]
+
+
+def l1_rel(a, b):
+    """Per variable: sum |a - b| / sum |b| over the physical zones."""
+    a, b = a[3:-3, 3:-3, 3:-3], b[3:-3, 3:-3, 3:-3]
+    return {nm: float(np.abs(a[..., l] - b[..., l]).sum() / max(np.abs(b[..., l]).sum(), 1e-300))
+            for l, nm in enumerate(VARS)}
+
+
+def mixed_form(args, wl, device, e64, p0, fp64_ms):
+    """The mixed-precision form on the same workload: its device time per
+    step, and after args.mixed_steps steps (and at a tenth of that) the
+    per-variable relative L1 difference from the FP64 run, beside the
+    difference a one-ulp change of u in the initial state makes to the FP64
+    run itself (how far the flow amplifies rounding)."""
+    em, _ = setup(wl, device, precision=1, p_init=p0)
+    em.step(args.warmup)
+    em.upload(p0)
+    em.set_time(em.desc.t, em.desc.dx[0])
+    em.step(args.steps)
+    mixed_ms = em.last_step_ms() / args.steps
+    K = args.mixed_steps
+    k1 = max(1, K // 10)
+    pert = p0.copy()
+    pert[..., 1] = np.nextafter(pert[..., 1], np.inf)
+    snaps = {}
+    for name, eng, start in (("fp64", e64, p0), ("mixed", em, p0), ("fp64_ulp", e64, pert)):
+        eng.upload(start)
+        eng.set_time(eng.desc.t, eng.desc.dx[0])
+        eng.step(k1)
+        a = eng.download()
+        eng.step(K - k1)
+        snaps[name] = (a, eng.download())
+    em.close()
+    zones = float(np.prod(wl["n"]))
+    res = {"value": zones / (mixed_ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": mixed_ms,
+           "speedup_vs_fp64": fp64_ms / mixed_ms, "dtype": "f32 reconstruction+flux, f64 elsewhere",
+           "accuracy": {}}
+    for idx, steps in ((0, k1), (1, K)):
+        res["accuracy"]["steps_%d" % steps] = {
+            "l1_rel_mixed_vs_fp64": l1_rel(snaps["mixed"][idx], snaps["fp64"][idx]),
+            "l1_rel_fp64_one_ulp": l1_rel(snaps["fp64_ulp"][idx], snaps["fp64"][idx])}
+    return res
 
 
 def reference_exe(cfg):

@@ -12,8 +12,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libharmgpu.so")
-SOURCES = ["hg_kernels.cu", "hg_api.cu", "hg_geometry.cu"]
-HEADERS = ["hg_internal.h", "hg_phys.cuh", "hg_fallback.cuh"]
+SOURCES = ["hg_kernels.cu", "hg_api.cu", "hg_geometry.cu", "hg_mixed.cu"]
+# FP32 kernels of the mixed-precision form may contract multiply-adds
+FMA_SOURCES = {"hg_mixed.cu"}
+HEADERS = ["hg_internal.h", "hg_phys.cuh", "hg_fallback.cuh", "hg_common.cuh"]
 
 
 def nvcc():
@@ -44,7 +46,10 @@ def build(force=False, verbose=False, out=None, defines=()):
     procs = []
     for s in SOURCES:
         o = os.path.join(CSRC, s.replace(".cu", ".o"))
-        cmd = [nvcc()] + flags() + ["-D" + d for d in defines] + ["-c", os.path.join(CSRC, s), "-o", o]
+        fl = flags()
+        if s in FMA_SOURCES:
+            fl = ["-fmad=true" if f == "-fmad=false" else f for f in fl]
+        cmd = [nvcc()] + fl + ["-D" + d for d in defines] + ["-c", os.path.join(CSRC, s), "-o", o]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((subprocess.Popen(cmd), s))

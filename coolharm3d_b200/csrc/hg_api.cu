@@ -106,7 +106,7 @@ static int validate(const hg_grid_desc *d)
   if (d->bc_type == 10 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
   if (d->metric_dim != 0 && d->metric_dim != 2) return HG_ERR_BADARG;
   if (d->cooling != 0 && d->cooling != 1) return HG_ERR_BADARG;
-  if (d->precision != HG_PREC_FP64) return HG_ERR_BADARG;
+  if (d->precision != HG_PREC_FP64 && d->precision != HG_PREC_MIXED) return HG_ERR_BADARG;
   // the tables of METRIC_DIM 2 vary with i and j: those directions must be resolved
   if (d->metric_dim == 2 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
   if (d->rescale_r && d->n1 == 1) return HG_ERR_BADARG;
@@ -145,6 +145,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
   h->ntot_ref = (long)h->NT[0] * h->NT[1] * h->NT[2];
   G.recon = desc->recon_type;
   G.flux = desc->flux_type;
+  G.prec = desc->precision;
   G.ct_para = desc->use_flux_ct_para;
   G.bc = desc->bc_type;
   G.mdim = desc->metric_dim;
@@ -187,6 +188,11 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
       ALLOC(G.conn, sizeof(double) * 64 * G.T[0] * G.T[1]);
     }
     if (G.rescale) ALLOC(G.rsc, sizeof(double) * 12 * G.T[0]);
+    if (G.prec == HG_PREC_MIXED) {
+      ALLOC(G.p32, sizeof(float) * HG_NPR * G.S);
+      if (G.mdim == 2) ALLOC(G.geomF, sizeof(float) * HG_GF * G.gS);
+      if (G.rescale) ALLOC(G.rsc32, sizeof(float) * 12 * G.T[0]);
+    }
     if (G.cooling) ALLOC(G.cool, sizeof(double) * 2 * G.T[0]);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device);
@@ -199,6 +205,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     };
     long faces = (long)G.T[0] * G.T[1] * G.T[2];
     h->L.grid_flux = grid_for(faces, 8);
+    h->L.grid_flux32 = grid_for(faces, 12);
     h->L.grid_emf = grid_for(faces, 8);
     h->L.grid_upd = grid_for(G.capacity, 8);
     h->L.grid_fix = grid_for(G.capacity, 4);
@@ -279,6 +286,21 @@ extern "C" int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom,
           for (int f = 0; f < 42; f++) t[f * G.gS + o] = s[f];
         }
     HG_CK(cudaMemcpy(G.geomT, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+    if (G.geomF) {  // the mixed form's FP32 face geometry
+      std::vector<float> f((size_t)HG_GF * G.gS);
+      for (long o = 0; o < G.gS; o++) {
+        for (int a = 0; a < 16; a++) f[a * G.gS + o] = (float)t[(16 + a) * G.gS + o];
+        f[16 * G.gS + o] = (float)t[0 * G.gS + o];
+        for (int j = 1; j <= 3; j++) {
+          f[(16 + j) * G.gS + o] = (float)t[j * G.gS + o];
+          f[(19 + j) * G.gS + o] = (float)t[(j * 4 + j) * G.gS + o];
+        }
+        f[23 * G.gS + o] = (float)t[38 * G.gS + o];
+        for (int a = 0; a < 3; a++) f[(24 + a) * G.gS + o] = (float)t[(35 + a) * G.gS + o];
+        f[27 * G.gS + o] = (float)t[32 * G.gS + o];
+      }
+      HG_CK(cudaMemcpy(G.geomF, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
+    }
     const long cS = (long)G.T[0] * G.T[1];
     std::vector<double> c((size_t)64 * cS, 0.);
     for (int i = 0; i < G.N[0]; i++)
@@ -330,6 +352,10 @@ extern "C" int hg_set_cell_data(hg_handle *h, const double *cell6, const double 
       for (int a = 0; a < 6; a++) r[(6 + a) * T0 + i] = 1 / r[a * T0 + i];
     }
     HG_CK(cudaMemcpy(G.rsc, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice));
+    if (G.rsc32) {
+      std::vector<float> r32(r.begin(), r.end());
+      HG_CK(cudaMemcpy(G.rsc32, r32.data(), sizeof(float) * r32.size(), cudaMemcpyHostToDevice));
+    }
   }
   h->have_cells = true;
   return HG_OK;

@@ -25,12 +25,22 @@ enum { NF_FLOOR = 0, NF_TMAX, NF_GAMMA_MAX, NF_GAMMA_CALC, NF_USE_FULL_INV, NF_U
        NF_UTOPRIM_EE, NF_USE_INTERP_PRIM, NF_USE_INTERP_V, NF_INTERP_PRIM, NF_INTERP_V };
 enum { PF_NONE = 0, PF_INTERP_V = 1, PF_INTERP_PRIM = 2 };
 
+// planes of the FP32 face geometry: gcov[16], gcon00, gcon0j (j=1..3),
+// gconjj (j=1..3), ncon0, beta[3], sqrt(-g)
+#define HG_GF 28
+
 struct Geom {
   double gcon[4][4];
   double gcov[4][4];
   double g, g_inv, alpha;
   double beta[3];
   double ncon[4];
+  // accessors shared with table-backed geometry (hg_phys.cuh GRef)
+  __host__ __device__ double cov(int a, int b) const { return gcov[a][b]; }
+  __host__ __device__ double con(int a, int b) const { return gcon[a][b]; }
+  __host__ __device__ double nc(int a) const { return ncon[a]; }
+  __host__ __device__ double bet(int a) const { return beta[a]; }
+  __host__ __device__ double det() const { return g; }
 };
 
 // Device-resident scalars of one grid (t, dx[0], reductions, failure flags).
@@ -57,6 +67,11 @@ struct GridDev {
   long S;            // plane size
   int NE[3];         // last physical index N+2
   int recon, flux, ct_para, bc, mdim, use_ee, cooling, rescale, nsd;
+  int prec;                  // HG_PREC_FP64 or HG_PREC_MIXED (FP32 face fluxes)
+  // HG_PREC_MIXED only: FP32 copy of the substep's input primitives (8
+  // planes of S), FP32 geometry of the faces (HG_GF planes of gS, metric_dim
+  // 2) and FP32 RESCALE_R factors (12 planes of T0)
+  float *p32, *geomF, *rsc32;
   double gam, cour;
   double dx[4], invdx[4];
   double startx[4], grid_length[4];
@@ -85,6 +100,7 @@ struct GridDev {
 // Fixed grid sizes of the step's kernels (grid-stride loops).
 struct LaunchCfg {
   int grid_flux, grid_emf, grid_upd, grid_fix, grid_bnd;
+  int grid_flux32;  // FP32 flux kernel of the mixed form (more resident blocks)
 };
 
 // Kernel classes timed by the optional event recorder.

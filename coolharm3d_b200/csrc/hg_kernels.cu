@@ -24,11 +24,12 @@
 #include <cstdio>
 #include <cstring>
 
+#include "harmgpu.h"
+#include "hg_common.cuh"
 #include "hg_fallback.cuh"
 
 namespace hg {
 
-#define HG_BLK 128
 #ifndef HG_UPD_MINB
 #define HG_UPD_MINB 1
 #endif
@@ -36,33 +37,12 @@ namespace hg {
 #define HG_FLUX_MINB 4
 #endif
 
-__device__ __forceinline__ int rs_type(int l) { return l == RHO ? 0 : (l == UU ? 2 : 1); }
-
 // (x * rscale) * (1/rscale): the value rescale_prims_r() leaves in p_h after
 // it scaled and unscaled it around the x1 reconstruction (recon.c:1168-1200).
 __device__ __forceinline__ double rs_roundtrip(const GridDev &G, double x, int l, int i)
 {
   const int t = rs_type(l);
   return (x * G.rsc[t * G.T[0] + i]) * G.rsc[(6 + t) * G.T[0] + i];
-}
-
-__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *dst)
-{
-  __shared__ double red[HG_BLK / 32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double w = __shfl_down_sync(0xffffffffu, v, o);
-    v = w > v ? w : v;
-  }
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double m = red[0];
-    for (int w = 1; w < HG_BLK / 32; w++) m = red[w] > m ? red[w] : m;
-    // the maximum only grows: skip the atomic when it cannot raise it
-    if (m > 0. && m > __longlong_as_double((long long)*(volatile unsigned long long *)dst))
-      atomicMax(dst, (unsigned long long)__double_as_longlong(m));
-  }
 }
 
 __device__ __forceinline__ double block_sum(double v)
@@ -98,15 +78,6 @@ __device__ __forceinline__ void book(const GridDev &G, int nf, int i, int j, int
 {
   atomicAdd(&G.nfail[nf * G.S + off3(G, i, j, k)], 1u);
   atomicAdd(&G.sc->nfailtot[nf], 1ull);
-}
-
-// FAIL_GAMMA_CALC at a face: the reference computes each face once per ghost
-// copy of a degenerate direction (numerical_flux's ranges), booking it once
-// per copy; mult is that number of copies.
-__device__ __forceinline__ void book_face(const GridDev &G, int i, int j, int k, unsigned int mult)
-{
-  atomicAdd(&G.nfail[NF_GAMMA_CALC * G.S + off3(G, i, j, k)], mult);
-  atomicAdd(&G.sc->nfailtot[NF_GAMMA_CALC], (unsigned long long)mult);
 }
 
 // fail(type, state != 0): pflag, failure flags, boundary flag
@@ -168,26 +139,6 @@ __device__ __forceinline__ void face_prims(const GridDev &G, const double *__res
 
 // ---------------------------------------------------------------------------
 // k_flux: F[d] on faces [lo, lo+n) (reference indices).
-// One component of primtoflux(pr, q, dir) (phys.c:28-63), same operations.
-__device__ __forceinline__ double flux_comp(const double *pr, const State &q, int dir, double gg, int l)
-{
-  const double eta_ucon = q.eta * q.ucon[dir];
-  const double bcon_dir = q.bcon[dir];
-  double f;
-  if (l == RHO) {
-    f = pr[RHO] * q.ucon[dir];
-  } else if (l <= U3) {
-    const int a = l - 1;  // UU -> 0, U1 -> 1, ...
-    double m = eta_ucon * q.ucov[a] - bcon_dir * q.bcov[a];
-    if (a == dir) m += q.ptot;
-    f = (l == UU) ? m + pr[RHO] * q.ucon[dir] : m;
-  } else {
-    const int a = l - 4;
-    f = q.bcon[a] * q.ucon[dir] - q.bcon[dir] * q.ucon[a];
-  }
-  return f * gg;
-}
-
 // HLL/LF flux of a face from its two states; writes the 8 components and
 // returns ctop.  Component by component, so no 32-value temporaries.
 __device__ __forceinline__ double face_flux(const GridDev &G, const double *pl, const double *pr, const Geom &g, int d,
@@ -1011,6 +962,9 @@ static inline void mark(EventRec *r, int cls, cudaStream_t s)
   r->n++;
 }
 
+void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const int *lo, const int *n, unsigned int mult);
+void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
+
 static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, int d,
                             EventRec *R)
 {
@@ -1033,6 +987,10 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
       }
     }
     mark(R, KC_FLUX, s);
+    if (G.prec == HG_PREC_MIXED) {
+      launch_flux_f32(G, L.grid_flux32, s, d, lo, n, mult);  // reads G.p32, filled from ph
+      return;
+    }
 #define HG_FLUX(RSV, MD, DD) k_flux<RSV, MD, DD><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
 #define HG_FLUX_D(RSV, MD) \
   if (d == 0) HG_FLUX(RSV, MD, 0); \
@@ -1056,6 +1014,7 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
   const double dtfac = sub == 0 ? 0.5 : 1.0;
   mark(R, KC_MISC, s);
   k_begin<<<1, 1, 0, s>>>(G.sc);
+  if (G.prec == HG_PREC_MIXED) launch_to_f32(G, L.grid_upd, s, ph);
   for (int d = 0; d < 3; d++) launch_flux_dir(G, L, s, ph, d, R);
   {
     int lo[3], n[3];
@@ -1142,6 +1101,7 @@ void launch_planes_to_ref(const GridDev &G, const LaunchCfg &L, cudaStream_t s, 
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d)
 {
   k_reset_max<<<1, 1, 0, s>>>(G.sc, d + 1);
+  if (G.prec == HG_PREC_MIXED) launch_to_f32(G, L.grid_upd, s, G.p);
   launch_flux_dir(G, L, s, G.p, d, nullptr);
 }
 

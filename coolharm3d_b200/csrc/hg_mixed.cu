@@ -1,0 +1,201 @@
+// hg_mixed.cu -- the FP32 flux kernel of the mixed-precision form
+// (hg_grid_desc.precision = HG_PREC_MIXED).
+//
+// Reconstruction (reconstruct_fast, recon.c:894-1103, with rescale_prims_r
+// for RESCALE_R), the face states (get_state), the characteristic speeds
+// (vchar_fast) and the HLL/LF flux (numerical_flux, step_ch.c:636-790) run
+// in FP32: each substep first rounds its input primitives to an FP32 copy
+// (k_to_f32), the face geometry comes from an FP32 table made once, and the
+// fluxes are widened to double on store.  Everything after the
+// flux -- flux-CT EMFs and the induction update, the geometric and cooling
+// source terms, the conserved update, con-to-prim and the fixups -- stays in
+// the FP64 kernels, so the state is FP64 and only the face fluxes carry FP32
+// rounding.
+//
+// This file is compiled with fused multiply-add enabled (the FP64 kernels
+// are not): the FP32 path is not bit-matched to the reference, and FMA is
+// both faster and more accurate.
+#include <cuda_runtime.h>
+
+#include "hg_common.cuh"
+
+namespace hg {
+
+#define HG_FLUX32_MINB 6
+
+// The face's geometry in float: the entries get_state and vchar_fast read
+// (gcov, three gcon entries, ncon^0, beta, sqrt(-g)).
+struct GeomF {
+  float gcov[4][4];
+  float gcon00, gcon0d, gcondd;
+  float ncon0, beta[3], g;
+  __device__ float cov(int a, int b) const { return gcov[a][b]; }
+  __device__ float con(int a, int b) const { return a == 0 ? (b == 0 ? gcon00 : gcon0d) : gcondd; }
+  __device__ float nc(int) const { return ncon0; }
+  __device__ float bet(int a) const { return beta[a]; }
+  __device__ float det() const { return g; }
+};
+
+// metric_dim 0: the one geometry of the grid, rounded; metric_dim 2: the
+// FP32 table built by hg_set_geometry (HG_GF planes, see hg_internal.h)
+template <int MDIM>
+__device__ __forceinline__ void geom_f32(const GridDev &G, int d, int i, int j, GeomF &f)
+{
+  const int js = d + 1;
+  if (MDIM == 0) {
+    const Geom &g = G.g0;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) f.gcov[a][b] = (float)g.gcov[a][b];
+    f.gcon00 = (float)g.gcon[0][0];
+    f.gcon0d = (float)g.gcon[0][js];
+    f.gcondd = (float)g.gcon[js][js];
+    f.ncon0 = (float)g.ncon[0];
+    f.beta[0] = (float)g.beta[0];
+    f.beta[1] = (float)g.beta[1];
+    f.beta[2] = (float)g.beta[2];
+    f.g = (float)g.g;
+  } else {
+    const int ii = G.deg[0] ? 0 : i, jj = G.deg[1] ? 0 : j;
+    const float *t = G.geomF + ((long)d * G.T[1] + jj) * G.T[0] + ii;
+    const long s = G.gS;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) f.gcov[a][b] = __ldg(t + (a * 4 + b) * s);
+    f.gcon00 = __ldg(t + 16 * s);
+    f.gcon0d = __ldg(t + (16 + js) * s);
+    f.gcondd = __ldg(t + (19 + js) * s);
+    f.ncon0 = __ldg(t + 23 * s);
+    f.beta[0] = __ldg(t + 24 * s);
+    f.beta[1] = __ldg(t + 25 * s);
+    f.beta[2] = __ldg(t + 26 * s);
+    f.g = __ldg(t + 27 * s);
+  }
+}
+
+// Left/right FP32 states of face (i,j,k) in direction d from the FP32 copy
+// of the primitives; RESCALE_R scales the x1 stencil by the per-zone
+// factors of rescale_prims_r and the face values back by the FACE1 factors.
+template <bool RS>
+__device__ __forceinline__ void face_prims_f32(const GridDev &G, int d, int i, int j, int k, float *pl, float *pr)
+{
+  const long o = off3(G, i, j, k);
+  const float *ph = G.p32;
+  if (G.deg[d]) {
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) pl[l] = pr[l] = __ldg(ph + l * G.S + o);
+    return;
+  }
+  const long st = G.st[d];
+#pragma unroll
+  for (int l = 0; l < HG_NPR; l++) {
+    float y[6];
+    const float *b = ph + l * G.S + o - 3 * st;
+#pragma unroll
+    for (int m = 0; m < 6; m++) y[m] = __ldg(b + m * st);
+    if (RS && d == 0) {
+      const int t = rs_type(l);
+#pragma unroll
+      for (int m = 0; m < 6; m++) y[m] *= __ldg(G.rsc32 + t * G.T[0] + i - 3 + m);
+    }
+    recon_face(G.recon, y, &pl[l], &pr[l]);
+    if (RS && d == 0) {
+      const float f = __ldg(G.rsc32 + (9 + rs_type(l)) * G.T[0] + i);
+      pl[l] *= f;
+      pr[l] *= f;
+    }
+  }
+}
+
+// FP32 copy of the substep's input primitives (all 8 planes, ghosts included)
+__global__ void __launch_bounds__(HG_BLK) k_to_f32(GridDev G, const double *__restrict__ src)
+{
+  const long total = (long)HG_NPR * G.S;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += stride) G.p32[t] = (float)src[t];
+}
+
+void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src)
+{
+  k_to_f32<<<grid, HG_BLK, 0, s>>>(G, src);
+}
+
+template <bool RS, int MDIM, int d>
+__global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_f32(const __grid_constant__ GridDev G, int lo0,
+                                                                    int lo1, int lo2, int n0, int n1, int n2,
+                                                                    unsigned int mult)
+{
+  const long total = (long)n0 * n1 * n2;
+  const int dim = d + 1;
+  const float gam = (float)G.gam;
+  double vmax = 0.;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = lo0 + (int)(t % n0);
+    const int j = lo1 + (int)((t / n0) % n1);
+    const int k = lo2 + (int)(t / ((long)n0 * n1));
+    const long o = off3(G, i, j, k);
+    float pl[HG_NPR], pr[HG_NPR];
+    face_prims_f32<RS>(G, d, i, j, k, pl, pr);
+    GeomF g;
+    geom_f32<MDIM>(G, d, i, j, g);
+    StateT<float> ql, qr;
+    if (get_state(pl, g, gam, ql)) book_face(G, i, j, k, mult);
+    if (get_state(pr, g, gam, qr)) book_face(G, i, j, k, mult);
+    float cmaxl, cminl, cmaxr, cminr;
+    vchar_fast(ql, g, dim, gam, &cmaxl, &cminl);
+    vchar_fast(qr, g, dim, gam, &cmaxr, &cminr);
+    const float cmax = fabsf(fmaxf(fmaxf(0.f, cmaxl), cmaxr));
+    const float cmin = fabsf(fmaxf(fmaxf(0.f, -cminl), -cminr));
+    const float ctop = fmaxf(cmin, cmax);
+    const float gg = g.g;
+    double *Fd = G.F[d];
+    if (G.flux == 1) {
+      const float inv = 1.f / (cmax + cmin + (float)HG_SMALL);
+      const float cc = cmax * cmin;
+#pragma unroll
+      for (int l = 0; l < HG_NPR; l++) {
+        const float Ul = flux_comp(pl, ql, 0, gg, l), Ur = flux_comp(pr, qr, 0, gg, l);
+        const float Fl = flux_comp(pl, ql, dim, gg, l), Fr = flux_comp(pr, qr, dim, gg, l);
+        Fd[l * G.S + o] = (double)((cmax * Fl + cmin * Fr - cc * (Ur - Ul)) * inv);
+      }
+    } else {
+#pragma unroll
+      for (int l = 0; l < HG_NPR; l++) {
+        const float Ul = flux_comp(pl, ql, 0, gg, l), Ur = flux_comp(pr, qr, 0, gg, l);
+        const float Fl = flux_comp(pl, ql, dim, gg, l), Fr = flux_comp(pr, qr, dim, gg, l);
+        Fd[l * G.S + o] = (double)(0.5f * (Fl + Fr - ctop * (Ur - Ul)));
+      }
+    }
+    if (d == 0 && G.bc == 10) {  // fix_flux(), bounds.c:2263-2275
+      double *fr = G.F[0] + RHO * G.S + o;
+      if (i == HG_NGH && *fr > 0) *fr = 0.;
+      if (i == G.NE[0] + 1 && *fr < 0) *fr = 0.;
+    }
+    if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
+      if ((double)ctop > vmax) vmax = (double)ctop;
+  }
+  block_max_atomic(vmax, &G.sc->maxs[d + 1]);
+}
+
+void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const int *lo, const int *n, unsigned int mult)
+{
+#define HG_F32(RSV, MD, DD) \
+  k_flux_f32<RSV, MD, DD><<<grid, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
+#define HG_F32_D(RSV, MD) \
+  if (d == 0) HG_F32(RSV, MD, 0); \
+  else if (d == 1) HG_F32(RSV, MD, 1); \
+  else HG_F32(RSV, MD, 2);
+  if (G.mdim == 0) {
+    if (G.rescale) { HG_F32_D(true, 0) }
+    else { HG_F32_D(false, 0) }
+  } else {
+    if (G.rescale) { HG_F32_D(true, 2) }
+    else { HG_F32_D(false, 2) }
+  }
+#undef HG_F32_D
+#undef HG_F32
+}
+
+}  // namespace hg

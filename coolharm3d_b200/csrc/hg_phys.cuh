@@ -24,10 +24,12 @@ namespace hg {
 #define HG_UTSQ_TOO_BIG 1.e20
 #define HG_FAIL_VAL 1.e30
 
-struct State {
-  double ucon[4], ucov[4], bcon[4], bcov[4];
-  double bsq, p, eta, ptot;
+template <class T>
+struct StateT {
+  T ucon[4], ucov[4], bcon[4], bcov[4];
+  T bsq, p, eta, ptot;
 };
+typedef StateT<double> State;
 
 __device__ __forceinline__ long off3(const GridDev &G, int i, int j, int k)
 {
@@ -65,11 +67,12 @@ __device__ __forceinline__ void load_geom(const GridDev &G, int pos, int i, int 
   g.ncon[3] = __ldg(t + 41 * s);
 }
 
-__device__ __forceinline__ void lower4(const double *v, const Geom &g, double *w)  // metric.c:338
+template <class T, class GT>
+__device__ __forceinline__ void lower4(const T *v, const GT &g, T *w)  // metric.c:338
 {
 #pragma unroll
   for (int a = 0; a < 4; a++)
-    w[a] = g.gcov[a][0] * v[0] + g.gcov[a][1] * v[1] + g.gcov[a][2] * v[2] + g.gcov[a][3] * v[3];
+    w[a] = g.cov(a, 0) * v[0] + g.cov(a, 1) * v[1] + g.cov(a, 2) * v[2] + g.cov(a, 3) * v[3];
 }
 
 __device__ __forceinline__ void raise4(const double *v, const Geom &g, double *w)  // metric.c:362
@@ -81,47 +84,50 @@ __device__ __forceinline__ void raise4(const double *v, const Geom &g, double *w
 
 // The gcov-weighted spatial quadratic form of gamma_calc (phys.c:249-255),
 // Utoprim_new_body's Bsq and utsq (utoprim_2d_fast.c:255-304).
-__device__ __forceinline__ double quad3(const Geom &g, double a, double b, double c)
+template <class T, class GT>
+__device__ __forceinline__ T quad3(const GT &g, T a, T b, T c)
 {
-  return g.gcov[1][1] * a * a + g.gcov[2][2] * b * b + g.gcov[3][3] * c * c +
-         2 * (g.gcov[1][2] * a * b + g.gcov[1][3] * a * c + g.gcov[2][3] * b * c);
+  return g.cov(1, 1) * a * a + g.cov(2, 2) * b * b + g.cov(3, 3) * c * c +
+         2 * (g.cov(1, 2) * a * b + g.cov(1, 3) * a * c + g.cov(2, 3) * b * c);
 }
 
-__device__ __forceinline__ int gamma_calc(const double *pr, const Geom &g, double *gamma)  // phys.c:244-270
+template <class T, class GT>
+__device__ __forceinline__ int gamma_calc(const T *pr, const GT &g, T *gamma)  // phys.c:244-270
 {
-  double qsq = quad3(g, pr[U1], pr[U2], pr[U3]);
-  if (qsq < 0.) {
-    if (fabs(qsq) > 1.E-10) {
-      *gamma = 1.;
+  T qsq = quad3(g, pr[U1], pr[U2], pr[U3]);
+  if (qsq < T(0)) {
+    if (fabs(qsq) > T(1.E-10)) {
+      *gamma = T(1);
       return 1;
     }
-    qsq = 1.E-10;
+    qsq = T(1.E-10);
   }
-  *gamma = sqrt(1. + qsq);
+  *gamma = sqrt(T(1) + qsq);
   return 0;
 }
 
 // get_state (phys.c:199), with ucon_calc (phys.c:216) and bcon_calc (phys.c:75).
 // Returns 1 if gamma_calc failed (the caller books FAIL_GAMMA_CALC).
-__device__ __forceinline__ int get_state(const double *pr, const Geom &g, double gam, State &q)
+template <class T, class GT>
+__device__ __forceinline__ int get_state(const T *pr, const GT &g, T gam, StateT<T> &q)
 {
-  double gamma;
+  T gamma;
   const int bad = gamma_calc(pr, g, &gamma);
-  q.ucon[0] = gamma * g.ncon[0];
-  q.ucon[1] = pr[U1] - q.ucon[0] * g.beta[0];
-  q.ucon[2] = pr[U2] - q.ucon[0] * g.beta[1];
-  q.ucon[3] = pr[U3] - q.ucon[0] * g.beta[2];
+  q.ucon[0] = gamma * g.nc(0);
+  q.ucon[1] = pr[U1] - q.ucon[0] * g.bet(0);
+  q.ucon[2] = pr[U2] - q.ucon[0] * g.bet(1);
+  q.ucon[3] = pr[U3] - q.ucon[0] * g.bet(2);
   lower4(q.ucon, g, q.ucov);
-  const double inv_ut = 1. / q.ucon[0];
+  const T inv_ut = T(1) / q.ucon[0];
   q.bcon[0] = pr[B1] * q.ucov[1] + pr[B2] * q.ucov[2] + pr[B3] * q.ucov[3];
   q.bcon[1] = (pr[B1] + q.bcon[0] * q.ucon[1]) * inv_ut;
   q.bcon[2] = (pr[B2] + q.bcon[0] * q.ucon[2]) * inv_ut;
   q.bcon[3] = (pr[B3] + q.bcon[0] * q.ucon[3]) * inv_ut;
   lower4(q.bcon, g, q.bcov);
   q.bsq = q.bcon[0] * q.bcov[0] + q.bcon[1] * q.bcov[1] + q.bcon[2] * q.bcov[2] + q.bcon[3] * q.bcov[3];
-  q.p = (gam - 1.) * pr[UU];
+  q.p = (gam - T(1)) * pr[UU];
   q.eta = q.p + pr[RHO] + pr[UU] + q.bsq;
-  q.ptot = q.p + 0.5 * q.bsq;
+  q.ptot = q.p + T(0.5) * q.bsq;
   return bad;
 }
 
@@ -153,24 +159,25 @@ __device__ __forceinline__ void primtoflux(const double *pr, const State &q, int
   for (int l = 0; l < HG_NPR; l++) f[l] *= g.g;
 }
 
-__device__ __forceinline__ void vchar_fast(const State &q, const Geom &g, int js, double gam, double *vmax,
-                                           double *vmin)  // phys.c:432-501
+template <class T, class GT>
+__device__ __forceinline__ void vchar_fast(const StateT<T> &q, const GT &g, int js, T gam, T *vmax,
+                                           T *vmin)  // phys.c:432-501
 {
-  double cms2 = (gam * q.p + q.bsq) / q.eta;
-  if (cms2 < 0.) cms2 = HG_SMALL;
-  else if (cms2 > 1.) cms2 = 1.;
-  const double Au2 = q.ucon[js] * q.ucon[js];
-  const double Bu2 = q.ucon[0] * q.ucon[0];
-  const double AuBu = q.ucon[js] * q.ucon[0];
-  const double A = Bu2 - (g.gcon[0][0] + Bu2) * cms2;
-  const double B = AuBu - (g.gcon[0][js] + AuBu) * cms2;
-  const double C = Au2 - (g.gcon[js][js] + Au2) * cms2;
-  double discr = B * B - A * C;
-  if (discr < 0.) discr = 0.;
+  T cms2 = (gam * q.p + q.bsq) / q.eta;
+  if (cms2 < T(0)) cms2 = T(HG_SMALL);
+  else if (cms2 > T(1)) cms2 = T(1);
+  const T Au2 = q.ucon[js] * q.ucon[js];
+  const T Bu2 = q.ucon[0] * q.ucon[0];
+  const T AuBu = q.ucon[js] * q.ucon[0];
+  const T A = Bu2 - (g.con(0, 0) + Bu2) * cms2;
+  const T B = AuBu - (g.con(0, js) + AuBu) * cms2;
+  const T C = Au2 - (g.con(js, js) + Au2) * cms2;
+  T discr = B * B - A * C;
+  if (discr < T(0)) discr = T(0);
   discr = sqrt(discr);
-  const double denom = 1. / A;
-  const double vp = -(-B + discr) * denom;
-  const double vm = -(-B - discr) * denom;
+  const T denom = T(1) / A;
+  const T vp = -(-B + discr) * denom;
+  const T vm = -(-B - discr) * denom;
   if (vp > vm) {
     *vmax = vp;
     *vmin = vm;
@@ -180,6 +187,27 @@ __device__ __forceinline__ void vchar_fast(const State &q, const Geom &g, int js
   }
 }
 
+// One component of primtoflux(pr, q, dir) (phys.c:28-63), same operations.
+template <class T>
+__device__ __forceinline__ T flux_comp(const T *pr, const StateT<T> &q, int dir, T gg, int l)
+{
+  const T eta_ucon = q.eta * q.ucon[dir];
+  const T bcon_dir = q.bcon[dir];
+  T f;
+  if (l == RHO) {
+    f = pr[RHO] * q.ucon[dir];
+  } else if (l <= U3) {
+    const int a = l - 1;  // UU -> 0, U1 -> 1, ...
+    T m = eta_ucon * q.ucov[a] - bcon_dir * q.bcov[a];
+    if (a == dir) m += q.ptot;
+    f = (l == UU) ? m + pr[RHO] * q.ucon[dir] : m;
+  } else {
+    const int a = l - 4;
+    f = q.bcon[a] * q.ucon[dir] - q.bcon[dir] * q.ucon[a];
+  }
+  return f * gg;
+}
+
 // ---------------------------------------------------------------------------
 // Reconstruction of one variable at one face from the six zones around it.
 // y[0..5] are zones f-3 .. f+2 along the direction; *yl is the left state
@@ -187,30 +215,32 @@ __device__ __forceinline__ void vchar_fast(const State &q, const Geom &g, int js
 // f, p_R[f]).  PPM: linear_recon_vect (recon.c:237-264) + para_vect
 // (recon.c:611-641); limiters: linear_recon (recon.c:86-125).
 
-__device__ __forceinline__ double slope_vect(int rt, double a, double b)  // recon.c:246-260
+template <class T>
+__device__ __forceinline__ T slope_vect(int rt, T a, T b)  // recon.c:246-260
 {
-  const double s = a * b;
-  if (s <= 0.) return 0.;
+  const T s = a * b;
+  if (s <= T(0)) return T(0);
   if (rt == 2 || rt == 5) {
-    const double a_abs = fabs(a), b_abs = fabs(b);
-    const double a3 = a_abs + a_abs + a_abs, b3 = b_abs + b_abs + b_abs;
+    const T a_abs = fabs(a), b_abs = fabs(b);
+    const T a3 = a_abs + a_abs + a_abs, b3 = b_abs + b_abs + b_abs;
     if (a3 <= b_abs) return a + a;
     if (b3 <= a_abs) return b + b;
-    return 0.5 * (a + b);
+    return T(0.5) * (a + b);
   }
   if (rt == 0 || rt == 3) return (fabs(a) <= fabs(b)) ? a : b;
-  return 2 * s / (a + b);
+  return T(2) * s / (a + b);
 }
 
-__device__ __forceinline__ void para_cell(double yi, double l, double r, double *lnew, double *rnew)  // recon.c:624-638
+template <class T>
+__device__ __forceinline__ void para_cell(T yi, T l, T r, T *lnew, T *rnew)  // recon.c:624-638
 {
-  const double qa = (r - yi) * (yi - l);
-  if (qa <= 0.) {
+  const T qa = (r - yi) * (yi - l);
+  if (qa <= T(0)) {
     *lnew = *rnew = yi;
     return;
   }
-  const double r2 = r + r, l2 = l + l, y3 = yi + yi + yi;
-  double ln = l, rn = r;
+  const T r2 = r + r, l2 = l + l, y3 = yi + yi + yi;
+  T ln = l, rn = r;
   if (r > l) {
     if (y3 > (l + r2)) ln = y3 - r2;
     if (y3 < (l2 + r)) rn = y3 - l2;
@@ -222,16 +252,17 @@ __device__ __forceinline__ void para_cell(double yi, double l, double r, double 
   *rnew = rn;
 }
 
-__device__ __forceinline__ double linear_recon(int rt, double y1, double y2, double y3)  // recon.c:86-125
+template <class T>
+__device__ __forceinline__ T linear_recon(int rt, T y1, T y2, T y3)  // recon.c:86-125
 {
-  double Dqm, Dqp, s;
+  T Dqm, Dqp, s;
   if (rt == 2) {
-    Dqm = 2. * (y2 - y1);
-    Dqp = 2. * (y3 - y2);
-    const double Dqc = 0.5 * (y3 - y1);
+    Dqm = T(2) * (y2 - y1);
+    Dqp = T(2) * (y3 - y2);
+    const T Dqc = T(0.5) * (y3 - y1);
     s = Dqm * Dqp;
-    if (s <= 0.) return 0.;
-    const double aDqm = fabs(Dqm), aDqp = fabs(Dqp), aDqc = fabs(Dqc);
+    if (s <= T(0)) return T(0);
+    const T aDqm = fabs(Dqm), aDqp = fabs(Dqp), aDqc = fabs(Dqc);
     if ((aDqm <= aDqp) && (aDqm <= aDqc)) return Dqm;
     if (aDqp <= aDqc) return Dqp;
     return Dqc;
@@ -239,28 +270,29 @@ __device__ __forceinline__ double linear_recon(int rt, double y1, double y2, dou
   Dqm = (y2 - y1);
   Dqp = (y3 - y2);
   s = Dqm * Dqp;
-  if (s <= 0.) return 0.;
+  if (s <= T(0)) return T(0);
   if (rt == 0) return (fabs(Dqm) < fabs(Dqp)) ? Dqm : Dqp;
-  return 2. * s / (Dqm + Dqp);
+  return T(2) * s / (Dqm + Dqp);
 }
 
 // PPM states at face f from y[0..5] = zones f-3 .. f+2: *yl = right edge of
 // zone f-1, *yr = left edge of zone f.  The slope limiter is the one of
 // linear_recon_vect for RECON_TYPE_CHOICE rt (also used by the EMF
 // reconstruction of flux_ct_para_fast2 whatever rt is).
-__device__ __forceinline__ void ppm_face(int rt, const double *y, double *yl, double *yr)
+template <class T>
+__device__ __forceinline__ void ppm_face(int rt, const T *y, T *yl, T *yr)
 {
   // slopes of zones f-2 .. f+1
-  const double d0 = y[1] - y[0], d1 = y[2] - y[1], d2 = y[3] - y[2], d3 = y[4] - y[3], d4 = y[5] - y[4];
-  const double q1 = slope_vect(rt, d0, d1);  // zone f-2
-  const double q2 = slope_vect(rt, d1, d2);  // zone f-1
-  const double q3 = slope_vect(rt, d2, d3);  // zone f
-  const double q4 = slope_vect(rt, d3, d4);  // zone f+1
+  const T d0 = y[1] - y[0], d1 = y[2] - y[1], d2 = y[3] - y[2], d3 = y[4] - y[3], d4 = y[5] - y[4];
+  const T q1 = slope_vect(rt, d0, d1);  // zone f-2
+  const T q2 = slope_vect(rt, d1, d2);  // zone f-1
+  const T q3 = slope_vect(rt, d2, d3);  // zone f
+  const T q4 = slope_vect(rt, d3, d4);  // zone f+1
   // face values between zones (f-2,f-1), (f-1,f), (f,f+1)
-  const double rA = 0.5 * (y[2] + y[1]) - HG_PPM_FACTOR * (q2 - q1);
-  const double rB = 0.5 * (y[3] + y[2]) - HG_PPM_FACTOR * (q3 - q2);
-  const double rC = 0.5 * (y[4] + y[3]) - HG_PPM_FACTOR * (q4 - q3);
-  double ln, rn;
+  const T rA = T(0.5) * (y[2] + y[1]) - T(HG_PPM_FACTOR) * (q2 - q1);
+  const T rB = T(0.5) * (y[3] + y[2]) - T(HG_PPM_FACTOR) * (q3 - q2);
+  const T rC = T(0.5) * (y[4] + y[3]) - T(HG_PPM_FACTOR) * (q4 - q3);
+  T ln, rn;
   para_cell(y[2], rA, rB, &ln, &rn);  // zone f-1
   *yl = rn;
   para_cell(y[3], rB, rC, &ln, &rn);  // zone f
@@ -268,13 +300,14 @@ __device__ __forceinline__ void ppm_face(int rt, const double *y, double *yl, do
 }
 
 // Face states from 6 zone values (y[0] = zone f-3).
-__device__ __forceinline__ void recon_face(int rt, const double *y, double *yl, double *yr)
+template <class T>
+__device__ __forceinline__ void recon_face(int rt, const T *y, T *yl, T *yr)
 {
   if (rt >= 3) {
     ppm_face(rt, y, yl, yr);
   } else {
-    const double dl = 0.5 * linear_recon(rt, y[1], y[2], y[3]);  // zone f-1
-    const double dr = 0.5 * linear_recon(rt, y[2], y[3], y[4]);  // zone f
+    const T dl = T(0.5) * linear_recon(rt, y[1], y[2], y[3]);  // zone f-1
+    const T dr = T(0.5) * linear_recon(rt, y[2], y[3], y[4]);  // zone f
     *yl = y[2] + dl;
     *yr = y[3] - dr;
   }
@@ -282,14 +315,15 @@ __device__ __forceinline__ void recon_face(int rt, const double *y, double *yl, 
 
 // PPM edge values of zone c on a line: *ln = left edge, *rn = right edge,
 // from y[0..4] = zones c-2 .. c+2 (the EMF reconstruction of flux_ct.c:759-939).
-__device__ __forceinline__ void ppm_zone(int rt, const double *y, double *ln, double *rn)
+template <class T>
+__device__ __forceinline__ void ppm_zone(int rt, const T *y, T *ln, T *rn)
 {
-  const double d0 = y[1] - y[0], d1 = y[2] - y[1], d2 = y[3] - y[2], d3 = y[4] - y[3];
-  const double q1 = slope_vect(rt, d0, d1);
-  const double q2 = slope_vect(rt, d1, d2);
-  const double q3 = slope_vect(rt, d2, d3);
-  const double l = 0.5 * (y[2] + y[1]) - HG_PPM_FACTOR * (q2 - q1);
-  const double r = 0.5 * (y[3] + y[2]) - HG_PPM_FACTOR * (q3 - q2);
+  const T d0 = y[1] - y[0], d1 = y[2] - y[1], d2 = y[3] - y[2], d3 = y[4] - y[3];
+  const T q1 = slope_vect(rt, d0, d1);
+  const T q2 = slope_vect(rt, d1, d2);
+  const T q3 = slope_vect(rt, d2, d3);
+  const T l = T(0.5) * (y[2] + y[1]) - T(HG_PPM_FACTOR) * (q2 - q1);
+  const T r = T(0.5) * (y[3] + y[2]) - T(HG_PPM_FACTOR) * (q3 - q2);
   para_cell(y[2], l, r, ln, rn);
 }
 
