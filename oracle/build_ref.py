@@ -106,6 +106,15 @@ CONFIGS = {
                ("rmax = 16. ;", "rmax = 12. ;"),
                ("  randfact = 0.;", "  randfact = 4.e-2;"),
                ("phys.c", "const double h_o_r  = 5.e-2;", "const double h_o_r  = 1.e-1;")]),
+    # Advected field loop (Gardiner & Stone 2005), 2D periodic Minkowski:
+    # PPM_MC + HLLE + para flux-CT, the shipped parameters.  The setup calls
+    # the time-dependent-coordinate macro SET_GEOM_COORD_TIME_FUNCS without
+    # including metric.h, where it is defined, so it does not link; the call
+    # (a no-op for the static Minkowski grid) is removed.
+    "field_loop": ("init.field_loop.c",
+                   dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)",
+                        RECON_TYPE_CHOICE="(RECON_PPM_MC)", FLUX_TYPE_CHOICE="(FLUX_HLLE)"),
+                   [("SET_GEOM_COORD_TIME_FUNCS(t,1);", "")]),
     # Same setup with van Leer PPM limiter and LF flux.
     "linwave_vl": ("init.linearwave.c",
                    dict(MINK, BC_TYPE_CHOICE="(BC_CARTESIAN_PERIODIC)",

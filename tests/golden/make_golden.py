@@ -45,6 +45,8 @@ CASES = [
     ("torus_24x16x8_s1", "torus", (24, 16, 8), 1, "load"),
     ("torus_24x16x8_s3", "torus", (24, 16, 8), 3, "load"),
     ("torus_stress_16x24x6_s1", "torus", (16, 24, 6), 1, 23),
+    # advected field loop, 2D periodic: the reference's own initial data
+    ("field_loop_24x24x1_s3", "field_loop", (24, 24, 1), 3, None),
 ]
 
 
@@ -117,5 +119,7 @@ def make(name, cfg, n, steps, seed):
 
 
 if __name__ == "__main__":
+    only = sys.argv[1:]
     for c in CASES:
-        make(*c)
+        if not only or c[0] in only:
+            make(*c)
