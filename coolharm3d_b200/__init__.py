@@ -45,7 +45,8 @@ EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", 
            "hg_upload_prims_tree", "hg_download_prims_tree", "hg_set_time", "hg_step", "hg_get_fail_counts",
            "hg_download_pflag", "hg_download_gamma", "hg_download_nfail", "hg_get_diag", "hg_last_step_ms",
            "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc", "hg_set_cooling_tables",
-           "hg_build_geometry_ks_mks", "hg_fixup_bounds"]
+           "hg_build_geometry_ks_mks", "hg_fixup_bounds", "hg_batch_create", "hg_batch_add", "hg_batch_remove",
+           "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 _lib = None
@@ -83,10 +84,18 @@ def load_library(path=LIB_PATH):
     lib.hg_face_flux_noalloc.argtypes = [ctypes.POINTER(GridDesc), P, P, P, P, ctypes.c_int32, P]
     D = ctypes.c_double
     lib.hg_fixup_bounds.argtypes = [P]
+    lib.hg_batch_create.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(P)]
+    lib.hg_batch_add.argtypes = [P, P]
+    lib.hg_batch_remove.argtypes = [P, P]
+    lib.hg_batch_size.argtypes = [P]
+    lib.hg_batch_step.argtypes = [P, P, P]
+    lib.hg_batch_destroy.argtypes = [P]
+    lib.hg_mem_info.argtypes = [ctypes.c_int32, P, P]
+    lib.hg_grid_bytes.argtypes = [ctypes.POINTER(GridDesc), P]
     lib.hg_build_geometry_ks_mks.argtypes = [ctypes.POINTER(GridDesc), D, D, D, D, ctypes.c_int32, D,
                                              P, P, P, P, P, P]
     for fn in EXPORTS:
-        if fn not in ("hg_destroy", "hg_strerror"):
+        if fn not in ("hg_destroy", "hg_strerror", "hg_batch_destroy"):
             getattr(lib, fn).restype = I
     _lib = lib
     return lib
@@ -264,3 +273,57 @@ class Engine:
         v = ctypes.c_double()
         _check(self.lib.hg_last_step_ms(self.h, ctypes.byref(v)), "hg_last_step_ms")
         return v.value
+
+
+def mem_info(device=0):
+    """(free, total) bytes of the device."""
+    f, t = ctypes.c_uint64(), ctypes.c_uint64()
+    _check(load_library().hg_mem_info(device, ctypes.byref(f), ctypes.byref(t)), "hg_mem_info")
+    return f.value, t.value
+
+
+def grid_bytes(desc):
+    """Device bytes hg_init allocates for desc."""
+    b = ctypes.c_uint64()
+    _check(load_library().hg_grid_bytes(ctypes.byref(desc), ctypes.byref(b)), "hg_grid_bytes")
+    return b.value
+
+
+class Batch:
+    """Resident grids of one device advanced together (hg_batch_*): one
+    step() advances every member by one of its own steps, its kernels
+    overlapping the other members' on the device."""
+
+    def __init__(self, device=0, max_grids=256):
+        self.lib = load_library()
+        b = ctypes.c_void_p()
+        _check(self.lib.hg_batch_create(device, max_grids, ctypes.byref(b)), "hg_batch_create")
+        self.b = b
+        self.members = []
+        self._t = np.zeros(max_grids)
+        self._dt = np.zeros(max_grids)
+
+    def add(self, engine):
+        _check(self.lib.hg_batch_add(self.b, engine.h), "hg_batch_add")
+        self.members.append(engine)
+
+    def remove(self, engine):
+        _check(self.lib.hg_batch_remove(self.b, engine.h), "hg_batch_remove")
+        self.members.remove(engine)
+
+    def __len__(self):
+        return len(self.members)
+
+    def step(self):
+        """One step of every member; returns (t, dt) arrays in member order."""
+        _check(self.lib.hg_batch_step(self.b, _ptr(self._t), _ptr(self._dt)), "hg_batch_step")
+        n = len(self.members)
+        return self._t[:n].copy(), self._dt[:n].copy()
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.hg_batch_destroy(self.b)
+            self.b = None
+            self.members = []
+
+    __del__ = close

@@ -20,6 +20,7 @@
 
 namespace hg {
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R);
+void *gather_times_kernel();
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d);
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
@@ -46,6 +47,9 @@ struct hg_handle {
   double *h_stage = nullptr;  // pinned transfer chunks (HG_XCH x HG_XCH_BYTES)
   cudaEvent_t xev[HG_XCH] = {};  // DMA completion of each transfer chunk
   double *d_ref = nullptr;    // device buffer in the reference layout, when F[0] is too small
+  cudaGraph_t step_graph = nullptr;  // one hg_step(1) captured for batches (hg_batch_*)
+  bool graph_dirty = true;           // the capture predates a change of the kernels' arguments
+  int batch_refs = 0;                // batches this grid belongs to
   long ntot_ref = 0;          // N1TOT*N2TOT*N3TOT of the reference layout
   int NT[3] = {0, 0, 0};      // reference extents
   // per-kernel-class timing (hg_profile)
@@ -65,16 +69,30 @@ struct hg_handle {
     }                                                                                 \
   } while (0)
 
+// a copy on the grid's stream, complete on return
+static cudaError_t copy_sync(hg_handle *h, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind)
+{
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return e;
+}
+
 // address of a field of the device-resident DevScalars (no host dereference)
 static void *sc_field(const GridDev &G, size_t off) { return (char *)G.sc + off; }
 
+// Every copy and memset of a grid goes through the grid's own stream: the
+// stream is non-blocking, so work on the legacy default stream (plain
+// cudaMemcpy / cudaMemset) would not be ordered before its kernels.
 static int dev_alloc(hg_handle *h, void **p, size_t bytes)
 {
   if (cudaMalloc(p, bytes) != cudaSuccess) {
     cudaGetLastError();
     return HG_ERR_NOMEM;
   }
-  cudaMemset(*p, 0, bytes);
+  if (cudaMemsetAsync(*p, 0, bytes, h->stream) != cudaSuccess) {
+    cudaFree(*p);
+    return HG_ERR_CUDA;
+  }
   h->allocs.push_back(*p);
   return HG_OK;
 }
@@ -169,6 +187,10 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     if ((rc = dev_alloc(h, &q_, (bytes))) != HG_OK) goto fail; \
     ptr = (decltype(ptr))q_;                                  \
   } while (0)
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return HG_ERR_CUDA;
+  }
   {
     ALLOC(G.p, S8 * HG_NPR);
     ALLOC(G.ph, S8 * HG_NPR);
@@ -216,8 +238,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
       rc = HG_ERR_NOMEM;
       goto fail;
     }
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
       rc = HG_ERR_CUDA;
       goto fail;
     }
@@ -230,7 +251,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     memset(&sc0, 0, sizeof(sc0));
     sc0.t = desc->t;
     sc0.dt = desc->dx[0];
-    if (cudaMemcpy(G.sc, &sc0, sizeof(sc0), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (copy_sync(h, G.sc, &sc0, sizeof(sc0), cudaMemcpyHostToDevice) != cudaSuccess) {
       rc = HG_ERR_CUDA;
       goto fail;
     }
@@ -246,11 +267,16 @@ fail:
 extern "C" void hg_destroy(hg_handle *h)
 {
   if (!h) return;
+  if (h->batch_refs > 0) {
+    fprintf(stderr, "libharmgpu: hg_destroy on a grid that is still in a batch; hg_batch_remove it first\n");
+    return;
+  }
   cudaSetDevice(h->d.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_stage) cudaFreeHost(h->h_stage);
+  if (h->step_graph) cudaGraphDestroy(h->step_graph);
   for (int x = 0; x < HG_XCH; x++)
     if (h->xev[x]) cudaEventDestroy(h->xev[x]);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -262,6 +288,7 @@ extern "C" void hg_destroy(hg_handle *h)
 extern "C" int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom, const double *conn, int64_t n_conn)
 {
   if (!h || !geom) return HG_ERR_BADARG;
+  h->graph_dirty = true;
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
   if (G.mdim == 0) {
@@ -285,7 +312,7 @@ extern "C" int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom,
           const long o = ((long)pos * G.T[1] + j) * G.T[0] + i;
           for (int f = 0; f < 42; f++) t[f * G.gS + o] = s[f];
         }
-    HG_CK(cudaMemcpy(G.geomT, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+    HG_CK(copy_sync(h, G.geomT, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
     if (G.geomF) {  // the mixed form's FP32 face geometry
       std::vector<float> f((size_t)HG_GF * G.gS);
       for (long o = 0; o < G.gS; o++) {
@@ -299,7 +326,7 @@ extern "C" int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom,
         for (int a = 0; a < 3; a++) f[(24 + a) * G.gS + o] = (float)t[(35 + a) * G.gS + o];
         f[27 * G.gS + o] = (float)t[32 * G.gS + o];
       }
-      HG_CK(cudaMemcpy(G.geomF, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
+      HG_CK(copy_sync(h, G.geomF, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
     }
     const long cS = (long)G.T[0] * G.T[1];
     std::vector<double> c((size_t)64 * cS, 0.);
@@ -309,7 +336,7 @@ extern "C" int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom,
         const long o = (long)(j + HG_NGH) * G.T[0] + (i + HG_NGH);
         for (int f = 0; f < 64; f++) c[f * cS + o] = s[f];
       }
-    HG_CK(cudaMemcpy(G.conn, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+    HG_CK(copy_sync(h, G.conn, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
   }
   h->have_geom = true;
   return HG_OK;
@@ -321,6 +348,7 @@ static inline int ref_of(const GridDev &G, int a, int x) { return G.deg[a] ? HG_
 extern "C" int hg_set_cell_data(hg_handle *h, const double *cell6, const double *rface)
 {
   if (!h || !cell6) return HG_ERR_BADARG;
+  h->graph_dirty = true;
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
   const int N2T = h->NT[1], N3T = h->NT[2];
@@ -333,7 +361,7 @@ extern "C" int hg_set_cell_data(hg_handle *h, const double *cell6, const double 
         fl[o] = cell6[r * 6 + 0];
         fl[G.S + o] = cell6[r * 6 + 1];
       }
-  HG_CK(cudaMemcpy(G.floors, fl.data(), sizeof(double) * fl.size(), cudaMemcpyHostToDevice));
+  HG_CK(copy_sync(h, G.floors, fl.data(), sizeof(double) * fl.size(), cudaMemcpyHostToDevice));
   if (G.rescale) {
     if (!rface) return HG_ERR_BADARG;
     const int T0 = G.T[0];
@@ -351,10 +379,10 @@ extern "C" int hg_set_cell_data(hg_handle *h, const double *cell6, const double 
       r[5 * T0 + i] = rloc;
       for (int a = 0; a < 6; a++) r[(6 + a) * T0 + i] = 1 / r[a * T0 + i];
     }
-    HG_CK(cudaMemcpy(G.rsc, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice));
+    HG_CK(copy_sync(h, G.rsc, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice));
     if (G.rsc32) {
       std::vector<float> r32(r.begin(), r.end());
-      HG_CK(cudaMemcpy(G.rsc32, r32.data(), sizeof(float) * r32.size(), cudaMemcpyHostToDevice));
+      HG_CK(copy_sync(h, G.rsc32, r32.data(), sizeof(float) * r32.size(), cudaMemcpyHostToDevice));
     }
   }
   h->have_cells = true;
@@ -372,7 +400,7 @@ extern "C" int hg_set_cooling_tables(hg_handle *h, const double *omega, const do
     c[i] = omega[i];
     c[T0 + i] = t_target[i];
   }
-  HG_CK(cudaMemcpy(h->G.cool, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+  HG_CK(copy_sync(h, h->G.cool, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
   h->have_cool = true;
   return HG_OK;
 }
@@ -553,7 +581,7 @@ extern "C" int hg_set_time(hg_handle *h, double t, double dt)
   if (!h) return HG_ERR_BADARG;
   HG_CK(cudaSetDevice(h->d.device));
   double v[2] = {t, dt};
-  HG_CK(cudaMemcpy(sc_field(h->G, offsetof(hg::DevScalars, t)), v, sizeof(v), cudaMemcpyHostToDevice));
+  HG_CK(copy_sync(h, sc_field(h->G, offsetof(hg::DevScalars, t)), v, sizeof(v), cudaMemcpyHostToDevice));
   return HG_OK;
 }
 
@@ -596,7 +624,7 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
     }
   }
   hg::DevScalars sc;
-  HG_CK(cudaMemcpy(&sc, h->G.sc, sizeof(sc), cudaMemcpyDeviceToHost));
+  HG_CK(copy_sync(h, &sc, h->G.sc, sizeof(sc), cudaMemcpyDeviceToHost));
   if (sc.err) return HG_ERR_DEVICE;
   if (t) *t = sc.t;
   if (dt) *dt = sc.dt;
@@ -626,7 +654,7 @@ extern "C" int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max
   HG_CK(cudaStreamSynchronize(h->stream));
   // per-cell planes -> reference layout with the variable index innermost
   std::vector<double> tmp((size_t)HG_NPR * G.S);
-  HG_CK(cudaMemcpy(tmp.data(), G.F[dir], sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
+  HG_CK(copy_sync(h, tmp.data(), G.F[dir], sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
   // faces numerical_flux() computes (step_ch.c:668-675), in reference indices
   int lo[3], hi[3];
   for (int a = 0; a < 3; a++) {
@@ -651,7 +679,7 @@ extern "C" int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max
       }
   if (max_char_speed) {
     unsigned long long m;
-    HG_CK(cudaMemcpy(&m, sc_field(G, offsetof(hg::DevScalars, maxs) + sizeof(unsigned long long) * (dir + 1)),
+    HG_CK(copy_sync(h, &m, sc_field(G, offsetof(hg::DevScalars, maxs) + sizeof(unsigned long long) * (dir + 1)),
                      sizeof(m), cudaMemcpyDeviceToHost));
     memcpy(max_char_speed, &m, sizeof(double));
   }
@@ -663,7 +691,7 @@ extern "C" int hg_get_fail_counts(hg_handle *h, uint64_t nfailtot[HG_NFAIL])
   if (!h || !nfailtot) return HG_ERR_BADARG;
   HG_CK(cudaSetDevice(h->d.device));
   unsigned long long v[16];
-  HG_CK(cudaMemcpy(v, sc_field(h->G, offsetof(hg::DevScalars, nfailtot)), sizeof(v), cudaMemcpyDeviceToHost));
+  HG_CK(copy_sync(h, v, sc_field(h->G, offsetof(hg::DevScalars, nfailtot)), sizeof(v), cudaMemcpyDeviceToHost));
   for (int l = 0; l < HG_NFAIL; l++) nfailtot[l] = v[l];
   return HG_OK;
 }
@@ -674,7 +702,7 @@ static int download_cellwise(hg_handle *h, const T *dsrc, T *out, int planes)
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
   std::vector<T> tmp((size_t)planes * G.S);
-  HG_CK(cudaMemcpy(tmp.data(), dsrc, sizeof(T) * tmp.size(), cudaMemcpyDeviceToHost));
+  HG_CK(copy_sync(h, tmp.data(), dsrc, sizeof(T) * tmp.size(), cudaMemcpyDeviceToHost));
   const long nref = h->ntot_ref;
   for (int pl = 0; pl < planes; pl++)
     for (int i = 0; i < h->NT[0]; i++)
@@ -709,7 +737,7 @@ extern "C" int hg_get_diag(hg_handle *h, double *m_tot, double mcs[3])
   if (!h) return HG_ERR_BADARG;
   HG_CK(cudaSetDevice(h->d.device));
   hg::DevScalars sc;
-  HG_CK(cudaMemcpy(&sc, h->G.sc, sizeof(sc), cudaMemcpyDeviceToHost));
+  HG_CK(copy_sync(h, &sc, h->G.sc, sizeof(sc), cudaMemcpyDeviceToHost));
   if (m_tot) *m_tot = sc.m_tot;
   if (mcs)
     for (int a = 0; a < 3; a++) mcs[a] = sc.last_maxs[a + 1];
@@ -775,5 +803,226 @@ extern "C" int hg_build_geometry_minkowski(const hg_grid_desc *d, double *geom, 
         c[4] = x2;
         c[5] = x3;
       }
+  return HG_OK;
+}
+
+// ===========================================================================
+// Batches: several resident grids of one device advanced together.  Each
+// member's step (the launch sequence of hg_step) is captured once into a
+// CUDA graph; the batch graph holds every member's graph as an independent
+// child node, so one graph launch runs all members' kernels concurrently,
+// followed by one kernel that gathers every member's t, dx[0] and error
+// status for a single small copy to the host.  The batch graph is rebuilt
+// when the membership changes or a member's captured step goes stale.
+// ===========================================================================
+struct hg_batch {
+  int device = 0, cap = 0;
+  std::vector<hg_handle *> members;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool dirty = true;
+  hg::DevScalars **d_sc = nullptr;  // device array of the members' DevScalars pointers
+  double *d_out = nullptr;          // 3 doubles per member: t, dt, err
+  double *h_out = nullptr;          // pinned copy
+};
+
+static int capture_step(hg_handle *h)
+{
+  if (h->step_graph && !h->graph_dirty) return HG_OK;
+  if (h->step_graph) {
+    cudaGraphDestroy(h->step_graph);
+    h->step_graph = nullptr;
+  }
+  HG_CK(cudaSetDevice(h->d.device));
+  HG_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  hg::launch_step(h->G, h->L, h->stream, nullptr);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  HG_CK(e);
+  HG_CK(cudaGetLastError());
+  h->step_graph = g;
+  h->graph_dirty = false;
+  return HG_OK;
+}
+
+static int batch_rebuild(hg_batch *b)
+{
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  const int n = (int)b->members.size();
+  if (n == 0) {
+    b->dirty = false;
+    return HG_OK;
+  }
+  std::vector<hg::DevScalars *> sc(n);
+  for (int m = 0; m < n; m++) {
+    int rc = capture_step(b->members[m]);
+    if (rc != HG_OK) return rc;
+    sc[m] = b->members[m]->G.sc;
+  }
+  HG_CK(cudaSetDevice(b->device));
+  HG_CK(cudaMemcpyAsync(b->d_sc, sc.data(), sizeof(void *) * n, cudaMemcpyHostToDevice, b->stream));
+  HG_CK(cudaStreamSynchronize(b->stream));
+  cudaGraph_t g = nullptr;
+  HG_CK(cudaGraphCreate(&g, 0));
+  std::vector<cudaGraphNode_t> kids(n);
+  cudaError_t e = cudaSuccess;
+  for (int m = 0; m < n && e == cudaSuccess; m++)
+    e = cudaGraphAddChildGraphNode(&kids[m], g, nullptr, 0, b->members[m]->step_graph);
+  if (e == cudaSuccess) {
+    hg::DevScalars **scp = b->d_sc;
+    int nn = n;
+    double *out = b->d_out;
+    void *args[] = {&scp, &nn, &out};
+    cudaKernelNodeParams kp = {};
+    kp.func = hg::gather_times_kernel();
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(128);
+    kp.kernelParams = args;
+    cudaGraphNode_t gather;
+    e = cudaGraphAddKernelNode(&gather, g, kids.data(), n, &kp);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+  cudaGraphDestroy(g);
+  HG_CK(e);
+  b->dirty = false;
+  return HG_OK;
+}
+
+extern "C" int hg_batch_create(int32_t device, int32_t max_grids, hg_batch **out)
+{
+  if (!out || max_grids < 1 || max_grids > 4096) return HG_ERR_BADARG;
+  *out = nullptr;
+  HG_CK(cudaSetDevice(device));
+  hg_batch *b = new (std::nothrow) hg_batch;
+  if (!b) return HG_ERR_NOMEM;
+  b->device = device;
+  b->cap = max_grids;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc((void **)&b->d_sc, sizeof(void *) * max_grids) != cudaSuccess ||
+      cudaMalloc((void **)&b->d_out, sizeof(double) * 3 * max_grids) != cudaSuccess ||
+      cudaMallocHost((void **)&b->h_out, sizeof(double) * 3 * max_grids) != cudaSuccess) {
+    cudaGetLastError();
+    hg_batch_destroy(b);
+    return HG_ERR_NOMEM;
+  }
+  *out = b;
+  return HG_OK;
+}
+
+extern "C" int hg_batch_add(hg_batch *b, hg_handle *h)
+{
+  if (!b || !h || h->d.device != b->device) return HG_ERR_BADARG;
+  if (!h->have_geom || !h->have_cells || !h->have_prims || (h->G.cooling && !h->have_cool)) return HG_ERR_STATE;
+  for (hg_handle *m : b->members)
+    if (m == h) return HG_ERR_BADARG;
+  if ((int)b->members.size() >= b->cap) return HG_ERR_NOMEM;
+  b->members.push_back(h);
+  h->batch_refs++;
+  b->dirty = true;
+  return HG_OK;
+}
+
+extern "C" int hg_batch_remove(hg_batch *b, hg_handle *h)
+{
+  if (!b || !h) return HG_ERR_BADARG;
+  for (size_t m = 0; m < b->members.size(); m++)
+    if (b->members[m] == h) {
+      b->members.erase(b->members.begin() + m);
+      h->batch_refs--;
+      b->dirty = true;
+      return HG_OK;
+    }
+  return HG_ERR_BADARG;
+}
+
+extern "C" int hg_batch_size(const hg_batch *b) { return b ? (int)b->members.size() : HG_ERR_BADARG; }
+
+extern "C" int hg_batch_step(hg_batch *b, double *t, double *dt)
+{
+  if (!b) return HG_ERR_BADARG;
+  HG_CK(cudaSetDevice(b->device));
+  for (hg_handle *m : b->members)
+    if (m->graph_dirty) b->dirty = true;
+  if (b->dirty) {
+    int rc = batch_rebuild(b);
+    if (rc != HG_OK) return rc;
+  }
+  const int n = (int)b->members.size();
+  if (n == 0) return HG_OK;
+  // work the members queued on their own streams (uploads, set_time) comes first
+  for (hg_handle *m : b->members) HG_CK(cudaStreamSynchronize(m->stream));
+  HG_CK(cudaGraphLaunch(b->exec, b->stream));
+  HG_CK(cudaMemcpyAsync(b->h_out, b->d_out, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, b->stream));
+  HG_CK(cudaStreamSynchronize(b->stream));
+  int rc = HG_OK;
+  for (int m = 0; m < n; m++) {
+    if (t) t[m] = b->h_out[3 * m];
+    if (dt) dt[m] = b->h_out[3 * m + 1];
+    if (b->h_out[3 * m + 2] != 0.) rc = HG_ERR_DEVICE;
+  }
+  return rc;
+}
+
+extern "C" void hg_batch_destroy(hg_batch *b)
+{
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (hg_handle *m : b->members) m->batch_refs--;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->d_sc) cudaFree(b->d_sc);
+  if (b->d_out) cudaFree(b->d_out);
+  if (b->h_out) cudaFreeHost(b->h_out);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+// ---------------------------------------------------------------------------
+extern "C" int hg_mem_info(int32_t device, uint64_t *free_bytes, uint64_t *total_bytes)
+{
+  size_t f = 0, t = 0;
+  HG_CK(cudaSetDevice(device));
+  HG_CK(cudaMemGetInfo(&f, &t));
+  if (free_bytes) *free_bytes = f;
+  if (total_bytes) *total_bytes = t;
+  return HG_OK;
+}
+
+// The device memory hg_init allocates for a description (the same planes
+// and tables), plus the reference-layout transfer buffer a grid with a
+// one-zone direction adds on its first transfer.
+extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
+{
+  if (!d || !bytes) return HG_ERR_BADARG;
+  int rc = validate(d);
+  if (rc) return rc;
+  const long n[3] = {d->n1, d->n2, d->n3};
+  long T[3], S = 1, NT = 1;
+  for (int a = 0; a < 3; a++) {
+    T[a] = n[a] == 1 ? 1 : n[a] + 2 * HG_NGH;
+    S *= T[a];
+    NT *= n[a] + 2 * HG_NGH;
+  }
+  const long cap = n[0] * n[1] * n[2];
+  const long gS = (long)HG_NPOS * T[0] * T[1];
+  uint64_t b = 0;
+  b += 8ull * HG_NPR * S * 5;                 // p, ph, F[3]
+  b += 8ull * S * 3 + 8ull * S + 4ull * S;    // emf[3], p_gamma, pflag
+  b += 4ull * S * HG_NF + 8ull * S * 2;       // nfail, floors
+  b += sizeof(hg::DevScalars) + 8ull * cap * (2 + HG_NPR);  // scalars, queue, flagged list
+  if (d->metric_dim == 2) b += 8ull * 42 * gS + 8ull * 64 * T[0] * T[1];
+  if (d->rescale_r) b += 8ull * 12 * T[0];
+  if (d->cooling) b += 8ull * 2 * T[0];
+  if (d->precision == HG_PREC_MIXED) {
+    b += 4ull * HG_NPR * S;
+    if (d->metric_dim == 2) b += 4ull * HG_GF * gS;
+    if (d->rescale_r) b += 4ull * 12 * T[0];
+  }
+  b += 8ull * 148 * 8;                        // per-block partials
+  if (NT > S) b += 8ull * HG_NPR * NT;        // transfer buffer of a grid with a one-zone direction
+  *bytes = b;
   return HG_OK;
 }

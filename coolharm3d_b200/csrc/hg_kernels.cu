@@ -1112,6 +1112,18 @@ void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
   k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0);
 }
 
+// t, dx[0] and the error status of every member of a batch, for one copy
+__global__ void k_gather_times(DevScalars *const *sc, int n, double *out)
+{
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    out[3 * m] = sc[m]->t;
+    out[3 * m + 1] = sc[m]->dt;
+    out[3 * m + 2] = (double)sc[m]->err;
+  }
+}
+
+void *gather_times_kernel() { return (void *)k_gather_times; }
+
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R)
 {
   launch_substep(G, L, s, 0, R);

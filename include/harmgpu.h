@@ -171,6 +171,34 @@ int hg_last_step_ms(hg_handle *h, double *ms);
 int hg_profile(hg_handle *h, int32_t enable);
 int hg_kernel_times(hg_handle *h, double ms[HG_NKCLASS], int64_t launches[HG_NKCLASS]);
 
+/* Batches: resident grids of one device advanced together (no reference
+ * counterpart; the reference runs one grid per process).  Each member's step
+ * is captured once into a CUDA graph (on the first hg_batch_step after it
+ * joins, and again after hg_set_geometry/hg_set_cell_data); one
+ * hg_batch_step launches every member's step as independent branches of one
+ * graph, so their kernels overlap on the device, and returns each member's
+ * t and dx[0] (arrays of hg_batch_size() entries, membership order = order
+ * of hg_batch_add, members removed close the gap).  A member is advanced by
+ * exactly the kernels hg_step(h, 1, ...) would run: its result is bit for bit
+ * the one it gets alone.  Members must have geometry, cell data and
+ * primitives (HG_ERR_STATE otherwise) and live on the batch's device; while
+ * a batch step runs, no member may be used otherwise.  hg_destroy refuses a
+ * grid that is still a member.  HG_ERR_NOMEM if max_grids members are
+ * already in; HG_ERR_DEVICE if a member's kernels reported an error. */
+/* Free and total memory of a device (cudaMemGetInfo), and the device memory
+ * hg_init will allocate for a description: what a server admitting grids by
+ * free memory needs.  No reference counterpart. */
+int hg_mem_info(int32_t device, uint64_t *free_bytes, uint64_t *total_bytes);
+int hg_grid_bytes(const hg_grid_desc *desc, uint64_t *bytes);
+
+typedef struct hg_batch hg_batch;
+int hg_batch_create(int32_t device, int32_t max_grids, hg_batch **out);
+int hg_batch_add(hg_batch *b, hg_handle *h);
+int hg_batch_remove(hg_batch *b, hg_handle *h);
+int hg_batch_size(const hg_batch *b);
+int hg_batch_step(hg_batch *b, double *t, double *dt);
+void hg_batch_destroy(hg_batch *b);
+
 void hg_destroy(hg_handle *h);
 const char *hg_strerror(int code);
 
