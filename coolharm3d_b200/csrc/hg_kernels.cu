@@ -211,6 +211,111 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux(const __grid_cons
 }
 
 // ---------------------------------------------------------------------------
+// k_flux_strip: the faces of a strided direction d (x2 or x3) in strips of
+// NF consecutive faces along d, one strip per thread, lanes along x1.  The
+// thread marches along its strip once per variable, so each zone's slope,
+// interface value and PPM edges are computed once per strip instead of once
+// for each of the faces that read them (reconstruct_fast computes them once
+// per zone as well).  The face states wait in shared memory, each thread in
+// its own column, until the strip's fluxes are formed.  Every face value is
+// produced by the same operations on the same inputs as in face_prims.
+#ifndef HG_STRIP_NF
+#define HG_STRIP_NF 2
+#endif
+
+// Face states of NF faces f0 .. f0+NF-1 along d from zones f0-3 .. f0+NF+1
+// of one variable; zones past the strip's nf faces are clamped (their
+// results are not used).  pl -> sm[bl + s], pr -> sm[br + s].
+template <bool RS, int NF>
+__device__ __forceinline__ void strip_recon(const GridDev &G, const double *__restrict__ col, long st, int l, int i,
+                                            int nf, double *sm, int bl, int br, int tx)
+{
+  const int rt = G.recon;
+  double y[NF + 5];
+#pragma unroll
+  for (int c = 0; c < NF + 5; c++) {
+    const int cc = c < nf + 4 ? c : nf + 4;
+    double v = __ldg(col + cc * st);
+    if (RS) v = rs_roundtrip(G, v, l, i);
+    y[c] = v;
+  }
+  if (rt >= 3) {
+    double q[NF + 4];  // q[c]: slope of zone c, c = 1 .. NF+3
+#pragma unroll
+    for (int c = 1; c <= NF + 3; c++) q[c] = slope_vect(rt, y[c] - y[c - 1], y[c + 1] - y[c]);
+    double I[NF + 3];  // I[c]: value at the interface of zones c and c+1, c = 1 .. NF+2
+#pragma unroll
+    for (int c = 1; c <= NF + 2; c++) I[c] = 0.5 * (y[c + 1] + y[c]) - HG_PPM_FACTOR * (q[c + 1] - q[c]);
+    // zones c = 2 .. NF+2: face s = c - 2 takes the right edge of zone c
+    // (its left state), face s = c - 3 the left edge (its right state)
+#pragma unroll
+    for (int c = 2; c <= NF + 2; c++) {
+      double ln, rn;
+      para_cell(y[c], I[c - 1], I[c], &ln, &rn);
+      if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = rn;
+      if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = ln;
+    }
+  } else {
+#pragma unroll
+    for (int c = 2; c <= NF + 2; c++) {
+      const double dq = 0.5 * linear_recon(rt, y[c - 1], y[c], y[c + 1]);
+      if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = y[c] + dq;
+      if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = y[c] - dq;
+    }
+  }
+}
+
+template <bool RS, int MDIM, int d, int NF>
+__global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux_strip(const __grid_constant__ GridDev G,
+                                                                   const double *__restrict__ ph, int lo0, int lo1,
+                                                                   int lo2, int n0, int n1, int n2, unsigned int mult)
+{
+  extern __shared__ double sm[];  // 16 * NF * HG_BLK doubles: the strip's face states
+  const int tx = threadIdx.x;
+  const int nd = (d == 1) ? n1 : n2;
+  const int nseg = (nd + NF - 1) / NF;
+  const int nother = (d == 1) ? n2 : n1;
+  const long total = (long)n0 * nseg * nother;
+  const long st = G.st[d];
+  double vmax = 0.;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = lo0 + (int)(t % n0);
+    const long rest = t / n0;
+    const int seg = (int)(rest % nseg);
+    const int other = (int)(rest / nseg);
+    const int f0 = (d == 1 ? lo1 : lo2) + seg * NF;
+    const int nf = min(NF, nd - seg * NF);
+    const int j0 = (d == 1) ? f0 : lo1 + other;
+    const int k0 = (d == 1) ? lo2 + other : f0;
+    const long o0 = off3(G, i, j0, k0);
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++)
+      strip_recon<RS, NF>(G, ph + l * G.S + o0 - 3 * st, st, l, i, nf, sm, 2 * NF * l, 2 * NF * l + NF, tx);
+    for (int s = 0; s < nf; s++) {
+      const int j = (d == 1) ? j0 + s : j0, k = (d == 2) ? k0 + s : k0;
+      double pl[HG_NPR], pr[HG_NPR];
+#pragma unroll
+      for (int l = 0; l < HG_NPR; l++) {
+        pl[l] = sm[(2 * NF * l + s) * HG_BLK + tx];
+        pr[l] = sm[(2 * NF * l + NF + s) * HG_BLK + tx];
+      }
+      const long o = o0 + s * st;
+      double ctop;
+      if (MDIM == 0) {
+        ctop = face_flux(G, pl, pr, G.g0, d, i, j, k, mult, G.F[d], o);
+      } else {
+        Geom g;
+        load_geom(G, d, i, j, g);
+        ctop = face_flux(G, pl, pr, g, d, i, j, k, mult, G.F[d], o);
+      }
+      if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
+        if (ctop > vmax) vmax = ctop;
+    }
+  }
+  block_max_atomic(vmax, &G.sc->maxs[d + 1]);
+}
+
+// ---------------------------------------------------------------------------
 // k_emf: corner EMFs at [lo, lo+n).
 // Right edge of zone c-1 and left edge of zone c on a line through the corner
 // (flux_ct.c:782-900 accumulate exactly these two into each corner).
@@ -963,6 +1068,25 @@ static inline void mark(EventRec *r, int cls, cudaStream_t s)
 }
 
 void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const int *lo, const int *n, unsigned int mult);
+
+// k_flux_strip keeps 16 * NF face states per thread in dynamic shared memory
+// (32 KiB per block for NF = 2; strips of 3 and 4 faces need the 48 KiB
+// limit raised, which is done once per instantiation, and measured slower:
+// their shared memory takes L1 capacity from the stencil loads).
+template <bool RS, int MDIM, int d>
+static void launch_strip(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, const int *lo,
+                         const int *n, unsigned int mult)
+{
+  const size_t smem = sizeof(double) * 16 * HG_STRIP_NF * HG_BLK;
+  static bool ready = false;
+  if (!ready) {
+    cudaFuncSetAttribute(k_flux_strip<RS, MDIM, d, HG_STRIP_NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    ready = true;
+  }
+  k_flux_strip<RS, MDIM, d, HG_STRIP_NF><<<L.grid_flux, HG_BLK, smem, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1],
+                                                                          n[2], mult);
+}
 void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
 
 static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, int d,
@@ -992,10 +1116,12 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
       return;
     }
 #define HG_FLUX(RSV, MD, DD) k_flux<RSV, MD, DD><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
+#define HG_STRIP(RSV, MD, DD) \
+  launch_strip<RSV, MD, DD>(G, L, s, ph, lo, n, mult)
 #define HG_FLUX_D(RSV, MD) \
   if (d == 0) HG_FLUX(RSV, MD, 0); \
-  else if (d == 1) HG_FLUX(RSV, MD, 1); \
-  else HG_FLUX(RSV, MD, 2);
+  else if (d == 1) { if (G.deg[1]) HG_FLUX(RSV, MD, 1); else HG_STRIP(RSV, MD, 1); } \
+  else { if (G.deg[2]) HG_FLUX(RSV, MD, 2); else HG_STRIP(RSV, MD, 2); }
     if (G.mdim == 0) {
       if (G.rescale) { HG_FLUX_D(true, 0) }
       else { HG_FLUX_D(false, 0) }
@@ -1004,6 +1130,7 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
       else { HG_FLUX_D(false, 2) }
     }
 #undef HG_FLUX_D
+#undef HG_STRIP
 #undef HG_FLUX
 }
 

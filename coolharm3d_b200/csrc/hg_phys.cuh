@@ -215,41 +215,40 @@ __device__ __forceinline__ T flux_comp(const T *pr, const StateT<T> &q, int dir,
 // f, p_R[f]).  PPM: linear_recon_vect (recon.c:237-264) + para_vect
 // (recon.c:611-641); limiters: linear_recon (recon.c:86-125).
 
+// Both limiters are written as selections among candidates computed up
+// front instead of early returns, so a warp takes no data-dependent branch;
+// every value selected is the one the reference's branch returns.
 template <class T>
 __device__ __forceinline__ T slope_vect(int rt, T a, T b)  // recon.c:246-260
 {
   const T s = a * b;
-  if (s <= T(0)) return T(0);
+  T r;
   if (rt == 2 || rt == 5) {
     const T a_abs = fabs(a), b_abs = fabs(b);
     const T a3 = a_abs + a_abs + a_abs, b3 = b_abs + b_abs + b_abs;
-    if (a3 <= b_abs) return a + a;
-    if (b3 <= a_abs) return b + b;
-    return T(0.5) * (a + b);
+    r = T(0.5) * (a + b);
+    r = (b3 <= a_abs) ? b + b : r;
+    r = (a3 <= b_abs) ? a + a : r;
+  } else if (rt == 0 || rt == 3) {
+    r = (fabs(a) <= fabs(b)) ? a : b;
+  } else {
+    r = T(2) * s / (a + b);
   }
-  if (rt == 0 || rt == 3) return (fabs(a) <= fabs(b)) ? a : b;
-  return T(2) * s / (a + b);
+  return (s <= T(0)) ? T(0) : r;
 }
 
 template <class T>
 __device__ __forceinline__ void para_cell(T yi, T l, T r, T *lnew, T *rnew)  // recon.c:624-638
 {
   const T qa = (r - yi) * (yi - l);
-  if (qa <= T(0)) {
-    *lnew = *rnew = yi;
-    return;
-  }
   const T r2 = r + r, l2 = l + l, y3 = yi + yi + yi;
-  T ln = l, rn = r;
-  if (r > l) {
-    if (y3 > (l + r2)) ln = y3 - r2;
-    if (y3 < (l2 + r)) rn = y3 - l2;
-  } else {
-    if (y3 < (l + r2)) ln = y3 - r2;
-    if (y3 > (l2 + r)) rn = y3 - l2;
-  }
-  *lnew = ln;
-  *rnew = rn;
+  const T cl = l + r2, cr = l2 + r;
+  const bool up = r > l;
+  const bool movel = up ? (y3 > cl) : (y3 < cl);
+  const bool mover = up ? (y3 < cr) : (y3 > cr);
+  const bool flat = qa <= T(0);
+  *lnew = flat ? yi : (movel ? y3 - r2 : l);
+  *rnew = flat ? yi : (mover ? y3 - l2 : r);
 }
 
 template <class T>
