@@ -194,6 +194,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
   {
     ALLOC(G.p, S8 * HG_NPR);
     ALLOC(G.ph, S8 * HG_NPR);
+    ALLOC(G.Uc, S8 * HG_NPR);
     for (int d = 0; d < 3; d++) ALLOC(G.F[d], S8 * HG_NPR);
     for (int d = 0; d < 3; d++) ALLOC(G.emf[d], S8);
     ALLOC(G.p_gamma, S8);
@@ -1009,7 +1010,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   const long cap = n[0] * n[1] * n[2];
   const long gS = (long)HG_NPOS * T[0] * T[1];
   uint64_t b = 0;
-  b += 8ull * HG_NPR * S * 5;                 // p, ph, F[3]
+  b += 8ull * HG_NPR * S * 6;                 // p, ph, Uc, F[3]
   b += 8ull * S * 3 + 8ull * S + 4ull * S;    // emf[3], p_gamma, pflag
   b += 4ull * S * HG_NF + 8ull * S * 2;       // nfail, floors
   b += sizeof(hg::DevScalars) + 8ull * cap * (2 + HG_NPR);  // scalars, queue, flagged list

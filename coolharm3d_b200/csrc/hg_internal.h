@@ -72,6 +72,7 @@ struct GridDev {
   // planes of S), FP32 geometry of the faces (HG_GF planes of gS, metric_dim
   // 2) and FP32 RESCALE_R factors (12 planes of T0)
   float *p32, *geomF, *rsc32;
+  double *Uc;                // conserved variables after the update (8 planes of S)
   double gam, cour;
   double dx[4], invdx[4];
   double startx[4], grid_length[4];

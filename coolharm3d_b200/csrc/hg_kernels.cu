@@ -8,10 +8,10 @@
 //               flux (numerical_flux, step_ch.c:636-790); the maximum
 //               characteristic speed is reduced per block into one atomic
 //   k_emf       corner EMFs of flux_ct_para_fast2 / flux_ct (flux_ct.c)
-//   k_update    conserved update with the geometric source and the CT
-//               corrected induction fluxes, then the 2D Newton inversion
-//               (advance, step_ch.c:312-399); zones that need the rest of
-//               the recover_primitives() tree are queued
+//   k_update_cons  conserved update with the geometric source and the CT
+//               corrected induction fluxes (advance, step_ch.c:312-370)
+//   k_update_c2p   the 2D Newton inversion (step_ch.c:371-399); zones that
+//               need the rest of the recover_primitives() tree are queued
 //   k_fallback  Utoprim_1d / entropy fix / floors for the queued zones
 //   k_bounds    ghost zones (bounds.c) and pflag ghosts
 //   k_fixup     fixup_interp_v / fixup_interp_prim over the flagged zones
@@ -30,8 +30,13 @@
 
 namespace hg {
 
-#ifndef HG_UPD_MINB
-#define HG_UPD_MINB 1
+// register caps of the two update kernels (4 blocks of 128 threads per SM;
+// measured best of 1-6 blocks on the torus)
+#ifndef HG_CONS_MINB
+#define HG_CONS_MINB 4
+#endif
+#ifndef HG_C2P_MINB
+#define HG_C2P_MINB 4
 #endif
 #ifndef HG_FLUX_MINB
 #define HG_FLUX_MINB 4
@@ -454,10 +459,18 @@ __device__ __forceinline__ void update_zone(const GridDev &G, int i, int j, int 
   U[B3] += Dt * (-(f0b3_p - f0b3_m) * G.invdx[1] - (f1b3_p - f1b3_m) * G.invdx[2] - (zero - zero) * G.invdx[3] + dU[B3]);
 }
 
-// k_update: every physical zone.  sub = 0 predictor (p_f = ph), 1 corrector (p_f = p).
+// The update of advance() (step_ch.c:312-399) in two kernels over every
+// physical zone, so that neither holds the geometry, the conserved-variable
+// sources and the Newton solver's state at once:
+//   k_update_cons  U(p_i), the geometric and cooling sources, the flux
+//                  divergence with the CT-corrected induction fluxes -> U
+//                  (the Uc planes) and the per-block M_tot partials;
+//   k_update_c2p   the 2D Newton inversion of U, the queue for the rest of
+//                  recover_primitives(), floors and gamma ceiling -> p_f.
+// sub = 0 predictor (p_f = ph), 1 corrector (p_f = p).
 template <bool RS, int MDIM>
-__global__ void __launch_bounds__(HG_BLK, HG_UPD_MINB) k_update(const __grid_constant__ GridDev G, int sub, double dtfac,
-                                                   const double *__restrict__ p_h, double *__restrict__ p_f)
+__global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __grid_constant__ GridDev G, int sub,
+                                                                    double dtfac, const double *__restrict__ p_h)
 {
   const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
   const long total = (long)N0 * N1 * N2;
@@ -465,7 +478,6 @@ __global__ void __launch_bounds__(HG_BLK, HG_UPD_MINB) k_update(const __grid_con
   const long S = G.S;
   const double *p = G.p;
   double msum = 0.;
-  unsigned int n_full = 0, n_floor = 0;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const int i = HG_NGH + (int)(t % N0);
     const int j = HG_NGH + (int)((t / N0) % N1);
@@ -474,11 +486,11 @@ __global__ void __launch_bounds__(HG_BLK, HG_UPD_MINB) k_update(const __grid_con
     Geom gl;
     if (MDIM != 0) load_geom(G, 3, i, j, gl);
     const Geom &g = (MDIM == 0) ? G.g0 : gl;
-    double pi[HG_NPR], U[HG_NPR], dU[HG_NPR], pg[HG_NPR];
+    double pi[HG_NPR], U[HG_NPR], dU[HG_NPR];
 #pragma unroll
     for (int l = 0; l < HG_NPR; l++) {
-      pg[l] = p[l * S + o];
-      pi[l] = RS ? rs_roundtrip(G, pg[l], l, i) : pg[l];
+      const double v = p[l * S + o];
+      pi[l] = RS ? rs_roundtrip(G, v, l, i) : v;
     }
     {  // U(p_i) at the start of the step (U_gf[0])
       State q;
@@ -498,11 +510,39 @@ __global__ void __launch_bounds__(HG_BLK, HG_UPD_MINB) k_update(const __grid_con
     }
     update_zone(G, i, j, k, Dt, dU, U);
     msum += U[0];
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) G.Uc[l * S + o] = U[l];
+  }
+  const double bs = block_sum(msum);
+  if (threadIdx.x == 0) G.blk[blockIdx.x] = bs;
+}
+
+template <bool RS, int MDIM>
+__global__ void __launch_bounds__(HG_BLK, HG_C2P_MINB) k_update_c2p(const __grid_constant__ GridDev G, int sub,
+                                                                   double *__restrict__ p_f)
+{
+  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
+  const long total = (long)N0 * N1 * N2;
+  const long S = G.S;
+  const double *p = G.p;
+  unsigned int n_full = 0, n_floor = 0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = HG_NGH + (int)(t % N0);
+    const int j = HG_NGH + (int)((t / N0) % N1);
+    const int k = HG_NGH + (int)(t / ((long)N0 * N1));
+    const long o = off3(G, i, j, k);
+    Geom gl;
+    if (MDIM != 0) load_geom(G, 3, i, j, gl);
+    const Geom &g = (MDIM == 0) ? G.g0 : gl;
+    double U[HG_NPR], pf[HG_NPR];
     // Newton guess: the predictor's p_f (= ph) holds the unscaled copy of p;
     // the corrector's p_f is p itself, rescaled in place by the predictor.
-    double pf[HG_NPR];
 #pragma unroll
-    for (int l = 0; l < HG_NPR; l++) pf[l] = (sub == 0) ? pg[l] : pi[l];
+    for (int l = 0; l < HG_NPR; l++) {
+      U[l] = G.Uc[l * S + o];
+      const double v = p[l * S + o];
+      pf[l] = (RS && sub == 1) ? rs_roundtrip(G, v, l, i) : v;
+    }
     double gamma = 0., bsq = 0.;
     const int ret = utoprim_2d(U, g, G.gam, pf, &gamma, &bsq);
     const bool ee = G.use_ee && ((pf[UU] < HG_BETA_MIN * bsq) || (pf[RHO] < HG_BETA_MIN * bsq));
@@ -540,8 +580,6 @@ __global__ void __launch_bounds__(HG_BLK, HG_UPD_MINB) k_update(const __grid_con
 #pragma unroll
     for (int l = 0; l < HG_NPR; l++) p_f[l * S + o] = pf[l];
   }
-  const double bs = block_sum(msum);
-  if (threadIdx.x == 0) G.blk[blockIdx.x] = bs;
   const unsigned int c_full = block_count(n_full);
   const unsigned int c_floor = block_count(n_floor);
   if (threadIdx.x == 0) {
@@ -1153,13 +1191,17 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
     k_emf<<<L.grid_emf, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2]);
   }
   mark(R, KC_UPDATE, s);
+#define HG_UPD(RSV, MD)                                                      \
+  k_update_cons<RSV, MD><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph); \
+  k_update_c2p<RSV, MD><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, pf)
   if (G.mdim == 0) {
-    if (G.rescale) k_update<true, 0><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
-    else k_update<false, 0><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+    if (G.rescale) { HG_UPD(true, 0); }
+    else { HG_UPD(false, 0); }
   } else {
-    if (G.rescale) k_update<true, 2><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
-    else k_update<false, 2><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+    if (G.rescale) { HG_UPD(true, 2); }
+    else { HG_UPD(false, 2); }
   }
+#undef HG_UPD
   mark(R, KC_FALLBACK, s);
   if (G.rescale) k_fallback<true><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
   else k_fallback<false><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);

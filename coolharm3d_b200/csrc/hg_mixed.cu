@@ -179,14 +179,136 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_f32(const __gri
   block_max_atomic(vmax, &G.sc->maxs[d + 1]);
 }
 
+// Strips of NF consecutive faces along a strided direction (x2, x3), lanes
+// along x1: each zone's PPM edges are formed once per strip (the FP64
+// k_flux_strip's scheme); the strip's face states wait in shared memory.
+#ifndef HG_STRIP32_NF
+#define HG_STRIP32_NF 3
+#endif
+
+template <int NF>
+__device__ __forceinline__ void strip_recon_f32(int rt, const float *__restrict__ col, long st, int nf, float *sm,
+                                                int bl, int br, int tx)
+{
+  float y[NF + 5];
+#pragma unroll
+  for (int c = 0; c < NF + 5; c++) y[c] = __ldg(col + (c < nf + 4 ? c : nf + 4) * st);
+  if (rt >= 3) {
+    float q[NF + 4];
+#pragma unroll
+    for (int c = 1; c <= NF + 3; c++) q[c] = slope_vect(rt, y[c] - y[c - 1], y[c + 1] - y[c]);
+    float I[NF + 3];
+#pragma unroll
+    for (int c = 1; c <= NF + 2; c++) I[c] = 0.5f * (y[c + 1] + y[c]) - float(HG_PPM_FACTOR) * (q[c + 1] - q[c]);
+#pragma unroll
+    for (int c = 2; c <= NF + 2; c++) {
+      float ln, rn;
+      para_cell(y[c], I[c - 1], I[c], &ln, &rn);
+      if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = rn;
+      if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = ln;
+    }
+  } else {
+#pragma unroll
+    for (int c = 2; c <= NF + 2; c++) {
+      const float dq = 0.5f * linear_recon(rt, y[c - 1], y[c], y[c + 1]);
+      if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = y[c] + dq;
+      if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = y[c] - dq;
+    }
+  }
+}
+
+// HLL/LF flux of one face from FP32 states; returns ctop
+template <int MDIM, int d>
+__device__ __forceinline__ float face_flux_f32(const GridDev &G, const float *pl, const float *pr, int i, int j, int k,
+                                               unsigned int mult, long o)
+{
+  const int dim = d + 1;
+  const float gam = (float)G.gam;
+  GeomF g;
+  geom_f32<MDIM>(G, d, i, j, g);
+  StateT<float> ql, qr;
+  if (get_state(pl, g, gam, ql)) book_face(G, i, j, k, mult);
+  if (get_state(pr, g, gam, qr)) book_face(G, i, j, k, mult);
+  float cmaxl, cminl, cmaxr, cminr;
+  vchar_fast(ql, g, dim, gam, &cmaxl, &cminl);
+  vchar_fast(qr, g, dim, gam, &cmaxr, &cminr);
+  const float cmax = fabsf(fmaxf(fmaxf(0.f, cmaxl), cmaxr));
+  const float cmin = fabsf(fmaxf(fmaxf(0.f, -cminl), -cminr));
+  const float ctop = fmaxf(cmin, cmax);
+  const float gg = g.g;
+  double *Fd = G.F[d];
+  if (G.flux == 1) {
+    const float inv = 1.f / (cmax + cmin + (float)HG_SMALL);
+    const float cc = cmax * cmin;
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) {
+      const float Ul = flux_comp(pl, ql, 0, gg, l), Ur = flux_comp(pr, qr, 0, gg, l);
+      const float Fl = flux_comp(pl, ql, dim, gg, l), Fr = flux_comp(pr, qr, dim, gg, l);
+      Fd[l * G.S + o] = (double)((cmax * Fl + cmin * Fr - cc * (Ur - Ul)) * inv);
+    }
+  } else {
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++) {
+      const float Ul = flux_comp(pl, ql, 0, gg, l), Ur = flux_comp(pr, qr, 0, gg, l);
+      const float Fl = flux_comp(pl, ql, dim, gg, l), Fr = flux_comp(pr, qr, dim, gg, l);
+      Fd[l * G.S + o] = (double)(0.5f * (Fl + Fr - ctop * (Ur - Ul)));
+    }
+  }
+  return ctop;
+}
+
+template <int MDIM, int d, int NF>
+__global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const __grid_constant__ GridDev G, int lo0,
+                                                                          int lo1, int lo2, int n0, int n1, int n2,
+                                                                          unsigned int mult)
+{
+  __shared__ float sm[16 * NF * HG_BLK];
+  const int tx = threadIdx.x;
+  const int nd = (d == 1) ? n1 : n2;
+  const int nseg = (nd + NF - 1) / NF;
+  const int nother = (d == 1) ? n2 : n1;
+  const long total = (long)n0 * nseg * nother;
+  const long st = G.st[d];
+  double vmax = 0.;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int i = lo0 + (int)(t % n0);
+    const long rest = t / n0;
+    const int seg = (int)(rest % nseg);
+    const int other = (int)(rest / nseg);
+    const int f0 = (d == 1 ? lo1 : lo2) + seg * NF;
+    const int nf = min(NF, nd - seg * NF);
+    const int j0 = (d == 1) ? f0 : lo1 + other;
+    const int k0 = (d == 1) ? lo2 + other : f0;
+    const long o0 = off3(G, i, j0, k0);
+#pragma unroll
+    for (int l = 0; l < HG_NPR; l++)
+      strip_recon_f32<NF>(G.recon, G.p32 + l * G.S + o0 - 3 * st, st, nf, sm, 2 * NF * l, 2 * NF * l + NF, tx);
+    for (int s = 0; s < nf; s++) {
+      const int j = (d == 1) ? j0 + s : j0, k = (d == 2) ? k0 + s : k0;
+      float pl[HG_NPR], pr[HG_NPR];
+#pragma unroll
+      for (int l = 0; l < HG_NPR; l++) {
+        pl[l] = sm[(2 * NF * l + s) * HG_BLK + tx];
+        pr[l] = sm[(2 * NF * l + NF + s) * HG_BLK + tx];
+      }
+      const float ctop = face_flux_f32<MDIM, d>(G, pl, pr, i, j, k, mult, o0 + s * st);
+      if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
+        if ((double)ctop > vmax) vmax = (double)ctop;
+    }
+  }
+  block_max_atomic(vmax, &G.sc->maxs[d + 1]);
+}
+
 void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const int *lo, const int *n, unsigned int mult)
 {
 #define HG_F32(RSV, MD, DD) \
   k_flux_f32<RSV, MD, DD><<<grid, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
+#define HG_S32(MD, DD) \
+  k_flux_strip_f32<MD, DD, HG_STRIP32_NF><<<grid, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
 #define HG_F32_D(RSV, MD) \
   if (d == 0) HG_F32(RSV, MD, 0); \
-  else if (d == 1) HG_F32(RSV, MD, 1); \
-  else HG_F32(RSV, MD, 2);
+  else if (d == 1) { if (G.deg[1]) HG_F32(RSV, MD, 1); else HG_S32(MD, 1); } \
+  else { if (G.deg[2]) HG_F32(RSV, MD, 2); else HG_S32(MD, 2); }
   if (G.mdim == 0) {
     if (G.rescale) { HG_F32_D(true, 0) }
     else { HG_F32_D(false, 0) }
@@ -195,6 +317,7 @@ void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const in
     else { HG_F32_D(false, 2) }
   }
 #undef HG_F32_D
+#undef HG_S32
 #undef HG_F32
 }
 
