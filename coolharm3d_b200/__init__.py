@@ -46,7 +46,8 @@ EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", 
            "hg_download_pflag", "hg_download_gamma", "hg_download_nfail", "hg_get_diag", "hg_last_step_ms",
            "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc", "hg_set_cooling_tables",
            "hg_build_geometry_ks_mks", "hg_fixup_bounds", "hg_batch_create", "hg_batch_add", "hg_batch_remove",
-           "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes"]
+           "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes",
+           "hg_get_totals"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 _lib = None
@@ -91,6 +92,7 @@ def load_library(path=LIB_PATH):
     lib.hg_batch_step.argtypes = [P, P, P]
     lib.hg_batch_destroy.argtypes = [P]
     lib.hg_mem_info.argtypes = [ctypes.c_int32, P, P]
+    lib.hg_get_totals.argtypes = [P, P, P, P]
     lib.hg_grid_bytes.argtypes = [ctypes.POINTER(GridDesc), P]
     lib.hg_build_geometry_ks_mks.argtypes = [ctypes.POINTER(GridDesc), D, D, D, D, ctypes.c_int32, D,
                                              P, P, P, P, P, P]
@@ -252,6 +254,14 @@ class Engine:
         m = ctypes.c_double()
         _check(self.lib.hg_face_flux(self.h, d, _ptr(f), ctypes.byref(m)), "hg_face_flux")
         return f, m.value
+
+    def totals(self):
+        """(U_tot[8], F_tot[3, 2, 8], max |div B|) of the last step (dump_ener)."""
+        u = np.zeros(8)
+        f = np.zeros((3, 2, 8))
+        m = ctypes.c_double()
+        _check(self.lib.hg_get_totals(self.h, _ptr(u), _ptr(f), ctypes.byref(m)), "hg_get_totals")
+        return u, f, m.value
 
     def diag(self):
         m = ctypes.c_double()

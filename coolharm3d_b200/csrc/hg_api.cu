@@ -23,6 +23,7 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
 void *gather_times_kernel();
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d);
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
+void launch_totals(const GridDev &G, const LaunchCfg &L, cudaStream_t s, double *part, double *out);
 void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
                           double *out);
 void launch_planes_to_ref(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *in, int NT0, int NT1,
@@ -49,6 +50,7 @@ struct hg_handle {
   double *d_ref = nullptr;    // device buffer in the reference layout, when F[0] is too small
   cudaGraph_t step_graph = nullptr;  // one hg_step(1) captured for batches (hg_batch_*)
   bool graph_dirty = true;           // the capture predates a change of the kernels' arguments
+  double *d_tot = nullptr;           // hg_get_totals: per-block partials and the result
   int batch_refs = 0;                // batches this grid belongs to
   long ntot_ref = 0;          // N1TOT*N2TOT*N3TOT of the reference layout
   int NT[3] = {0, 0, 0};      // reference extents
@@ -1025,5 +1027,27 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   b += 8ull * 148 * 8;                        // per-block partials
   if (NT > S) b += 8ull * HG_NPR * NT;        // transfer buffer of a grid with a one-zone direction
   *bytes = b;
+  return HG_OK;
+}
+
+extern "C" int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], double *divb_max)
+{
+  if (!h) return HG_ERR_BADARG;
+  if (!h->have_geom || !h->have_cells || !h->have_prims) return HG_ERR_STATE;
+  HG_CK(cudaSetDevice(h->d.device));
+  if (!h->d_tot) {
+    void *q = nullptr;
+    int rc = dev_alloc(h, &q, sizeof(double) * 57 * (h->L.grid_upd + 1));
+    if (rc != HG_OK) return rc;
+    h->d_tot = (double *)q;
+  }
+  double *out = h->d_tot + 57L * h->L.grid_upd;
+  hg::launch_totals(h->G, h->L, h->stream, h->d_tot, out);
+  HG_CK(cudaGetLastError());
+  double v[57];
+  HG_CK(copy_sync(h, v, out, sizeof(v), cudaMemcpyDeviceToHost));
+  if (U_tot) memcpy(U_tot, v, 8 * sizeof(double));
+  if (F_tot) memcpy(F_tot, v + 8, 48 * sizeof(double));
+  if (divb_max) *divb_max = v[56];
   return HG_OK;
 }

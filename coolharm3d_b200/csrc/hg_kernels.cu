@@ -1281,6 +1281,137 @@ void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
   k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0);
 }
 
+// ---------------------------------------------------------------------------
+// dump_ener()'s integrals (diag.c:704-815) of the last step and the largest
+// divb_calc() (diag.c:503-612), per block; k_totals_final sums the blocks in
+// order.  Layout of part / out: U[8], F[3][2][8] (direction, lower/upper
+// boundary plane, variable; the induction components after flux-CT, from
+// the EMFs as update_zone forms them), max |div B|.
+#define HG_TOT 57
+__device__ __forceinline__ double ct_flux(const GridDev &G, int d, int l, long o)
+{
+  const double fac = G.ct_para ? 0.125 : 0.5;
+  const double *E0 = G.emf[0], *E1 = G.emf[1], *E2 = G.emf[2];
+  const long si = G.st[0], sj = G.st[1], sk = G.st[2];
+  if (d == 0) {
+    if (l == B2) return 0. + fac * (E2[o] + E2[o + sj]);
+    if (l == B3) return 0. + (-fac) * (E1[o] + E1[o + sk]);
+    return 0.;
+  }
+  if (d == 1) {
+    if (l == B1) return 0. + (-fac) * (E2[o] + E2[o + si]);
+    if (l == B3) return 0. + fac * (E0[o] + E0[o + sk]);
+    return 0.;
+  }
+  if (l == B1) return 0. + fac * (E1[o] + E1[o + si]);
+  if (l == B2) return 0. + (-fac) * (E0[o] + E0[o + sj]);
+  return 0.;
+}
+
+__device__ __forceinline__ double divb_zone(const GridDev &G, int i, int j, int k)
+{
+  double f[3] = {0., 0., 0.};
+#pragma unroll
+  for (int di = -1; di <= 0; di++)
+#pragma unroll
+    for (int dj = -1; dj <= 0; dj++)
+#pragma unroll
+      for (int dk = -1; dk <= 0; dk++) {
+        const long o = off3(G, i + di, j + dj, k + dk);
+        double g;
+        if (G.mdim == 0) g = G.g0.g;
+        else g = G.geomT[32 * G.gS + ((long)3 * G.T[1] + (G.deg[1] ? 0 : j + dj)) * G.T[0] + (G.deg[0] ? 0 : i + di)];
+        const double b1 = G.p[B1 * G.S + o], b2 = G.p[B2 * G.S + o], b3 = G.p[B3 * G.S + o];
+        f[0] += (di == 0 ? b1 : -b1) * g;
+        f[1] += (dj == 0 ? b2 : -b2) * g;
+        f[2] += (dk == 0 ? b3 : -b3) * g;
+      }
+  double divb = 0.;
+  divb += f[0] * G.invdx[1];
+  divb += f[1] * G.invdx[2];
+  divb += f[2] * G.invdx[3];
+  divb *= 0.25;
+  return fabs(divb);
+}
+
+__global__ void __launch_bounds__(HG_BLK) k_totals(GridDev G, double *part)
+{
+  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
+  double u[HG_NPR], fs[48], dm = 0.;
+  for (int l = 0; l < HG_NPR; l++) u[l] = 0.;
+  for (int l = 0; l < 48; l++) fs[l] = 0.;
+  const long zones = (long)N0 * N1 * N2;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < zones; t += stride) {
+    const int i = HG_NGH + (int)(t % N0), j = HG_NGH + (int)((t / N0) % N1), k = HG_NGH + (int)(t / ((long)N0 * N1));
+    const long o = off3(G, i, j, k);
+    for (int l = 0; l < HG_NPR; l++) u[l] += G.Uc[l * G.S + o];
+    const double v = divb_zone(G, i, j, k);
+    dm = v > dm ? v : dm;
+  }
+  // boundary face planes: d = 0 (j,k), d = 1 (i,k), d = 2 (i,j)
+  const long n_a[3] = {(long)N1 * N2, (long)N0 * N2, (long)N0 * N1};
+  for (int d = 0; d < 3; d++)
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n_a[d]; t += stride) {
+      int i, j, k;
+      if (d == 0) { i = HG_NGH; j = HG_NGH + (int)(t % N1); k = HG_NGH + (int)(t / N1); }
+      else if (d == 1) { i = HG_NGH + (int)(t % N0); j = HG_NGH; k = HG_NGH + (int)(t / N0); }
+      else { i = HG_NGH + (int)(t % N0); j = HG_NGH + (int)(t / N0); k = HG_NGH; }
+      for (int side = 0; side < 2; side++) {
+        const int ii = (d == 0 && side) ? N0 + HG_NGH : i, jj = (d == 1 && side) ? N1 + HG_NGH : j;
+        const int kk = (d == 2 && side) ? N2 + HG_NGH : k;
+        const long o = off3(G, ii, jj, kk);
+        for (int l = 0; l < HG_NPR; l++)
+          fs[(d * 2 + side) * HG_NPR + l] += (l >= B1) ? ct_flux(G, d, l, o) : G.F[d][l * G.S + o];
+      }
+    }
+  for (int l = 0; l < HG_NPR; l++) {
+    const double b = block_sum(u[l]);
+    if (threadIdx.x == 0) part[blockIdx.x * HG_TOT + l] = b;
+  }
+  for (int l = 0; l < 48; l++) {
+    const double b = block_sum(fs[l]);
+    if (threadIdx.x == 0) part[blockIdx.x * HG_TOT + 8 + l] = b;
+  }
+  __shared__ double red[HG_BLK / 32];
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const double w = __shfl_down_sync(0xffffffffu, dm, s);
+    dm = w > dm ? w : dm;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dm;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = red[0];
+    for (int w = 1; w < HG_BLK / 32; w++) m = red[w] > m ? red[w] : m;
+    part[blockIdx.x * HG_TOT + 56] = m;
+  }
+}
+
+__global__ void k_totals_final(GridDev G, const double *part, int nblk, double *out)
+{
+  const int m = threadIdx.x;
+  if (m >= HG_TOT) return;
+  double s = 0.;
+  for (int b = 0; b < nblk; b++) {
+    const double v = part[b * HG_TOT + m];
+    if (m == 56) s = v > s ? v : s;
+    else s += v;
+  }
+  if (m < 8) s *= G.dx[1] * G.dx[2] * G.dx[3];
+  else if (m < 56) {
+    const int d = (m - 8) / 16;
+    s *= d == 0 ? G.dx[2] * G.dx[3] : d == 1 ? G.dx[1] * G.dx[3] : G.dx[1] * G.dx[2];
+  }
+  out[m] = s;
+}
+
+void launch_totals(const GridDev &G, const LaunchCfg &L, cudaStream_t s, double *part, double *out)
+{
+  k_totals<<<L.grid_upd, HG_BLK, 0, s>>>(G, part);
+  k_totals_final<<<1, 64, 0, s>>>(G, part, L.grid_upd, out);
+}
+
 // t, dx[0] and the error status of every member of a batch, for one copy
 __global__ void k_gather_times(DevScalars *const *sc, int n, double *out)
 {

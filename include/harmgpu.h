@@ -158,6 +158,17 @@ int hg_get_diag(hg_handle *h, double *m_tot, double max_char_speed[3]);
  * uploading initial data and computing fields that read ghost zones. */
 int hg_fixup_bounds(hg_handle *h);
 
+/* dump_ener()'s integrals of the last step, computed on the device
+ * (diag.c:704-815): U_tot[l] = dV times the sum over the physical zones of
+ * the last substep's conserved variables; F_tot[(d*2 + side)*8 + l] = the
+ * face area times the sum of the last substep's fluxes over the lower
+ * (side 0) and upper (side 1) boundary face planes of direction d, with the
+ * flux-CT induction fluxes; and the largest divb_calc() (diag.c:503-612)
+ * over the physical zones.  Sums are per block, then over blocks in order:
+ * deterministic, within rounding of the reference's sequential sums.  Any
+ * output may be NULL.  Meaningful after at least one hg_step. */
+int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], double *divb_max);
+
 /* Device time of the last hg_step call in milliseconds (CUDA events). */
 int hg_last_step_ms(hg_handle *h, double *ms);
 

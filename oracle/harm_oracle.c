@@ -1818,6 +1818,84 @@ void or_face_flux(or_ctx *c, int d, double *flux, double *mcs)
   *mcs = c->max_char_speed[d + 1];
 }
 
+/* dump_ener()'s integrals (diag.c:704-815) after a step: U_tot[l] = dV sum
+ * of the last substep's conserved variables over the physical zones, F_tot
+ * [d][side][l] = face area times the sum of the last substep's fluxes (after
+ * flux_ct) over each boundary face plane; and the largest divb_calc()
+ * (diag.c:503-612) over the physical zones. */
+static double divb_zone(or_ctx *c, int i, int j, int k)
+{
+  double det_g[8], b1[8], b2[8], b3[8];
+  int id = 0, di, dj, dk;
+  for (di = -1; di <= 0; di++)
+    for (dj = -1; dj <= 0; dj++)
+      for (dk = -1; dk <= 0; dk++) {
+        const long o = IX(c, i + di, j + dj, k + dk);
+        det_g[id] = G(c, i + di, j + dj, k + dk, 3)->g;
+        b1[id] = di == 0 ? c->p[o * NP + B1] : -c->p[o * NP + B1];
+        b2[id] = dj == 0 ? c->p[o * NP + B2] : -c->p[o * NP + B2];
+        b3[id] = dk == 0 ? c->p[o * NP + B3] : -c->p[o * NP + B3];
+        id++;
+      }
+  double divb = 0., f;
+  f = 0.;
+  for (id = 0; id < 8; id++) f += b1[id] * det_g[id];
+  divb += f * (1. / c->d.dx[1]);
+  f = 0.;
+  for (id = 0; id < 8; id++) f += b2[id] * det_g[id];
+  divb += f * (1. / c->d.dx[2]);
+  f = 0.;
+  for (id = 0; id < 8; id++) f += b3[id] * det_g[id];
+  divb += f * (1. / c->d.dx[3]);
+  divb *= 0.25;
+  return fabs(divb);
+}
+
+void or_totals(or_ctx *c, double *U_tot, double *F_tot, double *divb_max)
+{
+  int i, j, k, l;
+  const int s1 = NG, e1 = c->N1 + NG - 1, s2 = NG, e2 = c->N2 + NG - 1, s3 = NG, e3 = c->N3 + NG - 1;
+  const double dV = c->d.dx[1] * c->d.dx[2] * c->d.dx[3];
+  for (l = 0; l < NP; l++) U_tot[l] = 0.;
+  for (l = 0; l < 48; l++) F_tot[l] = 0.;
+  double m = 0.;
+  for (i = s1; i <= e1; i++)
+    for (j = s2; j <= e2; j++)
+      for (k = s3; k <= e3; k++) {
+        for (l = 0; l < NP; l++) U_tot[l] += c->Un[IX(c, i, j, k) * NP + l];
+        const double v = divb_zone(c, i, j, k);
+        if (v > m) m = v;
+      }
+  for (l = 0; l < NP; l++) U_tot[l] *= dV;
+  for (j = s2; j <= e2; j++)
+    for (k = s3; k <= e3; k++)
+      for (l = 0; l < NP; l++) {
+        F_tot[(0 * 2 + 0) * NP + l] += FX(c, IX(c, s1, j, k), 0, l);
+        F_tot[(0 * 2 + 1) * NP + l] += FX(c, IX(c, e1 + 1, j, k), 0, l);
+      }
+  for (i = s1; i <= e1; i++)
+    for (k = s3; k <= e3; k++)
+      for (l = 0; l < NP; l++) {
+        F_tot[(1 * 2 + 0) * NP + l] += FX(c, IX(c, i, s2, k), 1, l);
+        F_tot[(1 * 2 + 1) * NP + l] += FX(c, IX(c, i, e2 + 1, k), 1, l);
+      }
+  for (i = s1; i <= e1; i++)
+    for (j = s2; j <= e2; j++)
+      for (l = 0; l < NP; l++) {
+        F_tot[(2 * 2 + 0) * NP + l] += FX(c, IX(c, i, j, s3), 2, l);
+        F_tot[(2 * 2 + 1) * NP + l] += FX(c, IX(c, i, j, e3 + 1), 2, l);
+      }
+  for (l = 0; l < NP; l++) {
+    F_tot[(0 * 2 + 0) * NP + l] *= c->d.dx[2] * c->d.dx[3];
+    F_tot[(0 * 2 + 1) * NP + l] *= c->d.dx[2] * c->d.dx[3];
+    F_tot[(1 * 2 + 0) * NP + l] *= c->d.dx[1] * c->d.dx[3];
+    F_tot[(1 * 2 + 1) * NP + l] *= c->d.dx[1] * c->d.dx[3];
+    F_tot[(2 * 2 + 0) * NP + l] *= c->d.dx[1] * c->d.dx[2];
+    F_tot[(2 * 2 + 1) * NP + l] *= c->d.dx[1] * c->d.dx[2];
+  }
+  *divb_max = m;
+}
+
 /* init_data()'s fixup(p); bounds(p,0); (init.torus.c:205-215): fixup(),
  * fixup.c:8-33, with fixup1zone(), fixup.c:45-75 (floors, gamma ceiling) */
 void or_fixup_bounds(or_ctx *c)

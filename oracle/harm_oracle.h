@@ -66,6 +66,9 @@ void or_get_nfail(const or_ctx *c, int32_t *nfail);      /* [OR_NFAIL][NTOT] */
 void or_get_nfailtot(const or_ctx *c, uint64_t *nfailtot);
 void or_get_time(const or_ctx *c, double *t, double *dt, double *m_tot);
 void or_step(or_ctx *c, int nsteps);
+/* dump_ener() integrals of the last step and the largest divb_calc():
+ * U_tot[8], F_tot[3][2][8] (direction, lower/upper boundary, variable). */
+void or_totals(or_ctx *c, double *U_tot, double *F_tot, double *divb_max);
 /* fixup(p); bounds(p,0); as the setups' init_data() calls them. */
 void or_fixup_bounds(or_ctx *c);
 /* reconstruct_fast + numerical_flux of the current primitives: the fluxes of

@@ -152,6 +152,7 @@ def oracle_lib():
         lib.or_get_time.argtypes = [P, P, P, P]
         lib.or_step.argtypes = [P, ctypes.c_int]
         lib.or_fixup_bounds.argtypes = [P]
+        lib.or_totals.argtypes = [P, P, P, P]
         lib.or_face_flux.argtypes = [P, ctypes.c_int, P, P]
         lib.or_set_cooling.argtypes = [P, P, P]
         lib.or_ntot.restype = ctypes.c_long
@@ -207,6 +208,13 @@ class Oracle:
 
     def fixup_bounds(self):
         self.lib.or_fixup_bounds(self.h)
+
+    def totals(self):
+        u = np.zeros(8)
+        f = np.zeros((3, 2, 8))
+        m = ctypes.c_double()
+        self.lib.or_totals(self.h, _ptr(u), _ptr(f), ctypes.byref(m))
+        return u, f, m.value
 
     def download(self):
         p = np.empty(self.shape + (NP,))
