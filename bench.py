@@ -216,6 +216,8 @@ def run_ours(args, wl, rank, world, device):
     import coolharm3d_b200 as hg
     n = wl["n"]
     e, p0 = setup(wl, device)
+    # launch configuration measured on this grid's own state (restored after)
+    tuned, tune_before, tune_after = e.autotune(steps=3)
     zones = n[0] * n[1] * n[2]
     barrier, sync = lambda: None, lambda: None
     try:
@@ -273,7 +275,8 @@ def run_ours(args, wl, rank, world, device):
                        "zones": zones, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (state arrays of %.2f GB each)" % (
                            8 * 8 * np.prod(hg.ref_shape(n)) / 1e9),
-                       "e2e": "upload from host once + K x (hg_step(1) + nfailtot readback) + download once"})
+                       "e2e": "upload from host once + K x (hg_step(1) + nfailtot readback) + download once",
+                       "launch": dict(tuned.as_dict(), autotune_ms_per_step=[tune_before, tune_after])})
     # roofline of the dominant kernel class (live CUDA events on the engine stream)
     dom = max(("flux", "update", "emf"), key=lambda c: kt[c][0])
     avg_ms = kt[dom][0] / max(kt[dom][1], 1)

@@ -47,8 +47,19 @@ EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", 
            "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc", "hg_set_cooling_tables",
            "hg_build_geometry_ks_mks", "hg_fixup_bounds", "hg_batch_create", "hg_batch_add", "hg_batch_remove",
            "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes",
-           "hg_get_totals"]
+           "hg_get_totals", "hg_get_launch_config", "hg_set_launch_config", "hg_autotune"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
+
+class LaunchConfig(ctypes.Structure):
+    """hg_launch_config: blocks per launch of each kernel class and the
+    strip length of the x2/x3 flux kernels."""
+    _fields_ = [("grid_flux", ctypes.c_int32), ("grid_flux32", ctypes.c_int32), ("grid_emf", ctypes.c_int32),
+                ("grid_update", ctypes.c_int32), ("grid_fixup", ctypes.c_int32), ("grid_bounds", ctypes.c_int32),
+                ("strip_faces", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
 
 _lib = None
 
@@ -93,6 +104,9 @@ def load_library(path=LIB_PATH):
     lib.hg_batch_destroy.argtypes = [P]
     lib.hg_mem_info.argtypes = [ctypes.c_int32, P, P]
     lib.hg_get_totals.argtypes = [P, P, P, P]
+    lib.hg_get_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
+    lib.hg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
+    lib.hg_autotune.argtypes = [P, ctypes.c_int32, ctypes.POINTER(LaunchConfig), P, P]
     lib.hg_grid_bytes.argtypes = [ctypes.POINTER(GridDesc), P]
     lib.hg_build_geometry_ks_mks.argtypes = [ctypes.POINTER(GridDesc), D, D, D, D, ctypes.c_int32, D,
                                              P, P, P, P, P, P]
@@ -254,6 +268,22 @@ class Engine:
         m = ctypes.c_double()
         _check(self.lib.hg_face_flux(self.h, d, _ptr(f), ctypes.byref(m)), "hg_face_flux")
         return f, m.value
+
+    def launch_config(self):
+        c = LaunchConfig()
+        _check(self.lib.hg_get_launch_config(self.h, ctypes.byref(c)), "hg_get_launch_config")
+        return c
+
+    def set_launch_config(self, c):
+        _check(self.lib.hg_set_launch_config(self.h, ctypes.byref(c)), "hg_set_launch_config")
+
+    def autotune(self, steps=3):
+        """Measure launch configurations on the resident state (which is
+        restored) and keep the fastest; returns (config, ms before, ms after)."""
+        c = LaunchConfig()
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.hg_autotune(self.h, steps, ctypes.byref(c), ctypes.byref(a), ctypes.byref(b)), "hg_autotune")
+        return c, a.value, b.value
 
     def totals(self):
         """(U_tot[8], F_tot[3, 2, 8], max |div B|) of the last step (dump_ener)."""

@@ -225,17 +225,21 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
       long g = (work + 127) / 128;
       long cap = (long)sms * per_sm;
       if (g > cap) g = cap;
+      if (g > HG_BLK_CAP) g = HG_BLK_CAP;
       if (g < 1) g = 1;
       return (int)g;
     };
     long faces = (long)G.T[0] * G.T[1] * G.T[2];
-    h->L.grid_flux = grid_for(faces, 8);
-    h->L.grid_flux32 = grid_for(faces, 12);
-    h->L.grid_emf = grid_for(faces, 8);
-    h->L.grid_upd = grid_for(G.capacity, 8);
-    h->L.grid_fix = grid_for(G.capacity, 4);
-    h->L.grid_bnd = grid_for(faces - G.capacity, 8);
-    ALLOC(G.blk, sizeof(double) * h->L.grid_upd);
+    // defaults from hg_autotune on the 192x192x128 torus: many short-lived
+    // blocks for the stencil and update kernels, few for the sparse lists
+    h->L.grid_flux = grid_for(faces, 64);
+    h->L.grid_flux32 = grid_for(faces, 96);
+    h->L.grid_emf = grid_for(faces, 64);
+    h->L.grid_upd = grid_for(G.capacity, 128);
+    h->L.grid_fix = grid_for(G.capacity, 2);
+    h->L.grid_bnd = grid_for(faces - G.capacity, 16);
+    h->L.strip_nf = 2;
+    ALLOC(G.blk, sizeof(double) * HG_BLK_CAP);
     if (cudaMallocHost((void **)&h->h_stage, (size_t)HG_XCH * HG_XCH_BYTES) != cudaSuccess) {
       cudaGetLastError();
       rc = HG_ERR_NOMEM;
@@ -1037,11 +1041,11 @@ extern "C" int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], do
   HG_CK(cudaSetDevice(h->d.device));
   if (!h->d_tot) {
     void *q = nullptr;
-    int rc = dev_alloc(h, &q, sizeof(double) * 57 * (h->L.grid_upd + 1));
+    int rc = dev_alloc(h, &q, sizeof(double) * 57 * (2048 + 1));
     if (rc != HG_OK) return rc;
     h->d_tot = (double *)q;
   }
-  double *out = h->d_tot + 57L * h->L.grid_upd;
+  double *out = h->d_tot + 57L * 2048;
   hg::launch_totals(h->G, h->L, h->stream, h->d_tot, out);
   HG_CK(cudaGetLastError());
   double v[57];
@@ -1049,5 +1053,202 @@ extern "C" int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], do
   if (U_tot) memcpy(U_tot, v, 8 * sizeof(double));
   if (F_tot) memcpy(F_tot, v + 8, 48 * sizeof(double));
   if (divb_max) *divb_max = v[56];
+  return HG_OK;
+}
+
+// ===========================================================================
+// Launch configuration and its autotuner.
+// ===========================================================================
+static bool config_ok(const hg_launch_config *c)
+{
+  const int32_t g[6] = {c->grid_flux, c->grid_flux32, c->grid_emf, c->grid_update, c->grid_fixup, c->grid_bounds};
+  for (int a = 0; a < 6; a++)
+    if (g[a] < 1 || g[a] > HG_BLK_CAP) return false;
+  return c->strip_faces >= 1 && c->strip_faces <= 3;
+}
+
+extern "C" int hg_get_launch_config(hg_handle *h, hg_launch_config *c)
+{
+  if (!h || !c) return HG_ERR_BADARG;
+  const hg::LaunchCfg &L = h->L;
+  *c = hg_launch_config{L.grid_flux, L.grid_flux32, L.grid_emf, L.grid_upd, L.grid_fix, L.grid_bnd, L.strip_nf, 0};
+  return HG_OK;
+}
+
+extern "C" int hg_set_launch_config(hg_handle *h, const hg_launch_config *c)
+{
+  if (!h || !c || !config_ok(c)) return HG_ERR_BADARG;
+  hg::LaunchCfg &L = h->L;
+  L.grid_flux = c->grid_flux;
+  L.grid_flux32 = c->grid_flux32;
+  L.grid_emf = c->grid_emf;
+  L.grid_upd = c->grid_update;
+  L.grid_fix = c->grid_fixup;
+  L.grid_bnd = c->grid_bounds;
+  L.strip_nf = c->strip_faces;
+  h->graph_dirty = true;
+  return HG_OK;
+}
+
+// The resident state a step changes, saved and put back around trial steps.
+struct Snapshot {
+  double *p = nullptr, *gam = nullptr;
+  int *pflag = nullptr;
+  unsigned int *nfail = nullptr;
+  hg::DevScalars *sc = nullptr;
+};
+
+static int snap(hg_handle *h, Snapshot &s, bool save)
+{
+  GridDev &G = h->G;
+  const size_t S8 = sizeof(double) * G.S;
+  if (save) {
+    if (cudaMalloc(&s.p, S8 * HG_NPR) != cudaSuccess || cudaMalloc(&s.gam, S8) != cudaSuccess ||
+        cudaMalloc(&s.pflag, sizeof(int) * G.S) != cudaSuccess ||
+        cudaMalloc(&s.nfail, sizeof(unsigned int) * G.S * HG_NF) != cudaSuccess ||
+        cudaMalloc(&s.sc, sizeof(hg::DevScalars)) != cudaSuccess) {
+      cudaGetLastError();
+      return HG_ERR_NOMEM;
+    }
+  }
+  auto cp = [&](void *a, void *b, size_t n) {  // save: device -> snapshot; else snapshot -> device
+    return save ? cudaMemcpyAsync(a, b, n, cudaMemcpyDeviceToDevice, h->stream)
+                : cudaMemcpyAsync(b, a, n, cudaMemcpyDeviceToDevice, h->stream);
+  };
+  HG_CK(cp(s.p, G.p, S8 * HG_NPR));
+  HG_CK(cp(s.gam, G.p_gamma, S8));
+  HG_CK(cp(s.pflag, G.pflag, sizeof(int) * G.S));
+  HG_CK(cp(s.nfail, G.nfail, sizeof(unsigned int) * G.S * HG_NF));
+  HG_CK(cp(s.sc, G.sc, sizeof(hg::DevScalars)));
+  HG_CK(cudaStreamSynchronize(h->stream));
+  return HG_OK;
+}
+
+static void snap_free(Snapshot &s)
+{
+  cudaFree(s.p);
+  cudaFree(s.gam);
+  cudaFree(s.pflag);
+  cudaFree(s.nfail);
+  cudaFree(s.sc);
+}
+
+// Per-class device time of `steps` steps from the snapshot under L.
+static int trial(hg_handle *h, Snapshot &s, int steps, double ms[HG_NKCLASS])
+{
+  int rc = snap(h, s, false);
+  if (rc != HG_OK) return rc;
+  const bool prof = h->prof;
+  h->prof = true;
+  for (int c = 0; c < HG_NKCLASS; c++) {
+    h->kc_ms[c] = 0.;
+    h->kc_n[c] = 0;
+  }
+  rc = hg_step(h, steps, nullptr, nullptr);
+  h->prof = prof;
+  for (int c = 0; c < HG_NKCLASS; c++) ms[c] = h->kc_ms[c];
+  return rc;
+}
+
+extern "C" int hg_autotune(hg_handle *h, int32_t steps, hg_launch_config *best, double *ms_before, double *ms_after)
+{
+  if (!h || steps < 1) return HG_ERR_BADARG;
+  if (!h->have_geom || !h->have_cells || !h->have_prims || (h->G.cooling && !h->have_cool)) return HG_ERR_STATE;
+  HG_CK(cudaSetDevice(h->d.device));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->d.device);
+  GridDev &G = h->G;
+  const long faces = (long)G.T[0] * G.T[1] * G.T[2];
+  auto grid_for = [&](long work, int per_sm) {
+    long g = (work + 127) / 128, cap = (long)sms * per_sm;
+    g = g > cap ? cap : g;
+    g = g > HG_BLK_CAP ? HG_BLK_CAP : g;
+    return (int)(g < 1 ? 1 : g);
+  };
+  const double sv_ms[HG_NKCLASS] = {0};
+  double sv_kc[HG_NKCLASS];
+  long long sv_kn[HG_NKCLASS];
+  memcpy(sv_kc, h->kc_ms, sizeof(sv_kc));
+  memcpy(sv_kn, h->kc_n, sizeof(sv_kn));
+  (void)sv_ms;
+  Snapshot s;
+  int rc = snap(h, s, true);
+  if (rc != HG_OK) {
+    snap_free(s);
+    return rc;
+  }
+  const hg::LaunchCfg start = h->L;
+  double ms[HG_NKCLASS];
+  auto total = [&](const double *m) {
+    double t = 0.;
+    for (int c = 0; c < HG_NKCLASS; c++) t += m[c];
+    return t;
+  };
+  rc = trial(h, s, steps, ms);  // first run pays one-time costs
+  if (rc == HG_OK) rc = trial(h, s, steps, ms);
+  const double t0 = total(ms);
+  hg::LaunchCfg L = start;
+  // one kernel class at a time, every candidate from the same state
+  const int mults[8] = {2, 4, 8, 16, 32, 64, 128, 1 << 20};  // blocks per SM; the last: one item per thread
+  auto pick = [&](int cls, auto apply) {
+    double bt = 1e300;
+    hg::LaunchCfg bl = L;
+    for (int a = 0; a < 8 && rc == HG_OK; a++)
+      for (int nf = 1; nf <= 3 && rc == HG_OK; nf++) {
+        hg::LaunchCfg c = L;
+        if (!apply(c, mults[a], nf)) continue;
+        h->L = c;
+        rc = trial(h, s, steps, ms);
+        if (rc == HG_OK && ms[cls] < bt) {
+          bt = ms[cls];
+          bl = c;
+        }
+      }
+    L = bl;
+  };
+  pick(hg::KC_FLUX, [&](hg::LaunchCfg &c, int m, int nf) {
+    c.grid_flux = grid_for(faces, m);
+    c.grid_flux32 = grid_for(faces, m + m / 2);
+    c.strip_nf = nf;
+    return true;
+  });
+  pick(hg::KC_EMF, [&](hg::LaunchCfg &c, int m, int nf) {
+    c.grid_emf = grid_for(faces, m);
+    return nf == 1;
+  });
+  pick(hg::KC_UPDATE, [&](hg::LaunchCfg &c, int m, int nf) {
+    c.grid_upd = grid_for(G.capacity, m);
+    return nf == 1;
+  });
+  pick(hg::KC_FALLBACK, [&](hg::LaunchCfg &c, int m, int nf) {
+    c.grid_fix = grid_for(G.capacity, m / 2);
+    return nf == 1;
+  });
+  pick(hg::KC_BOUNDS, [&](hg::LaunchCfg &c, int m, int nf) {
+    c.grid_bnd = grid_for(faces - G.capacity, m);
+    return nf == 1;
+  });
+  double t1 = t0;
+  if (rc == HG_OK) {
+    h->L = L;
+    rc = trial(h, s, steps, ms);
+    t1 = total(ms);
+    if (rc == HG_OK && t1 > t0) {  // keep the starting configuration if nothing beat it
+      h->L = start;
+      t1 = t0;
+    }
+  } else {
+    h->L = start;
+  }
+  const int rc2 = snap(h, s, false);
+  snap_free(s);
+  memcpy(h->kc_ms, sv_kc, sizeof(sv_kc));
+  memcpy(h->kc_n, sv_kn, sizeof(sv_kn));
+  h->graph_dirty = true;
+  if (rc != HG_OK) return rc;
+  if (rc2 != HG_OK) return rc2;
+  if (best) hg_get_launch_config(h, best);
+  if (ms_before) *ms_before = t0 / steps;
+  if (ms_after) *ms_after = t1 / steps;
   return HG_OK;
 }

@@ -102,7 +102,9 @@ struct GridDev {
 struct LaunchCfg {
   int grid_flux, grid_emf, grid_upd, grid_fix, grid_bnd;
   int grid_flux32;  // FP32 flux kernel of the mixed form (more resident blocks)
+  int strip_nf;     // faces per thread of the strided-direction flux kernels (1..3)
 };
+#define HG_BLK_CAP 65536  // largest grid of any kernel (the per-block M_tot partials are sized for it)
 
 // Kernel classes timed by the optional event recorder.
 enum { KC_FLUX = 0, KC_EMF, KC_UPDATE, KC_FALLBACK, KC_BOUNDS, KC_FIXUP, KC_MISC, KC_END, KC_N };

@@ -1106,26 +1106,35 @@ static inline void mark(EventRec *r, int cls, cudaStream_t s)
 }
 
 void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const int *lo, const int *n, unsigned int mult);
+void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
 
 // k_flux_strip keeps 16 * NF face states per thread in dynamic shared memory
-// (32 KiB per block for NF = 2; strips of 3 and 4 faces need the 48 KiB
-// limit raised, which is done once per instantiation, and measured slower:
-// their shared memory takes L1 capacity from the stencil loads).
+// (16, 32 and 48 KiB per block for NF = 1, 2, 3; the limit is raised once
+// per instantiation).  Longer strips save reconstruction work but their
+// shared memory takes L1 capacity from the stencil loads: on the 192^3-class
+// torus NF = 2 measured best, and hg_autotune chooses per grid.
+template <bool RS, int MDIM, int d, int NF>
+static void launch_strip_nf(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, const int *lo,
+                            const int *n, unsigned int mult)
+{
+  const size_t smem = sizeof(double) * 16 * NF * HG_BLK;
+  static bool ready = false;
+  if (!ready) {
+    cudaFuncSetAttribute(k_flux_strip<RS, MDIM, d, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ready = true;
+  }
+  k_flux_strip<RS, MDIM, d, NF><<<L.grid_flux, HG_BLK, smem, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult);
+}
+
+// strips of L.strip_nf faces (1, 2 or 3: a launch-configuration choice)
 template <bool RS, int MDIM, int d>
 static void launch_strip(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, const int *lo,
                          const int *n, unsigned int mult)
 {
-  const size_t smem = sizeof(double) * 16 * HG_STRIP_NF * HG_BLK;
-  static bool ready = false;
-  if (!ready) {
-    cudaFuncSetAttribute(k_flux_strip<RS, MDIM, d, HG_STRIP_NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    ready = true;
-  }
-  k_flux_strip<RS, MDIM, d, HG_STRIP_NF><<<L.grid_flux, HG_BLK, smem, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1],
-                                                                          n[2], mult);
+  if (L.strip_nf <= 1) launch_strip_nf<RS, MDIM, d, 1>(G, L, s, ph, lo, n, mult);
+  else if (L.strip_nf == 2) launch_strip_nf<RS, MDIM, d, 2>(G, L, s, ph, lo, n, mult);
+  else launch_strip_nf<RS, MDIM, d, 3>(G, L, s, ph, lo, n, mult);
 }
-void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
 
 static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, int d,
                             EventRec *R)
@@ -1288,6 +1297,7 @@ void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
 // boundary plane, variable; the induction components after flux-CT, from
 // the EMFs as update_zone forms them), max |div B|.
 #define HG_TOT 57
+#define HG_TOT_BLOCKS 2048  // blocks of k_totals at most (its partials array)
 __device__ __forceinline__ double ct_flux(const GridDev &G, int d, int l, long o)
 {
   const double fac = G.ct_para ? 0.125 : 0.5;
@@ -1408,8 +1418,9 @@ __global__ void k_totals_final(GridDev G, const double *part, int nblk, double *
 
 void launch_totals(const GridDev &G, const LaunchCfg &L, cudaStream_t s, double *part, double *out)
 {
-  k_totals<<<L.grid_upd, HG_BLK, 0, s>>>(G, part);
-  k_totals_final<<<1, 64, 0, s>>>(G, part, L.grid_upd, out);
+  const int nb = L.grid_upd < HG_TOT_BLOCKS ? L.grid_upd : HG_TOT_BLOCKS;
+  k_totals<<<nb, HG_BLK, 0, s>>>(G, part);
+  k_totals_final<<<1, 64, 0, s>>>(G, part, nb, out);
 }
 
 // t, dx[0] and the error status of every member of a batch, for one copy

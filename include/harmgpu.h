@@ -169,6 +169,25 @@ int hg_fixup_bounds(hg_handle *h);
  * output may be NULL.  Meaningful after at least one hg_step. */
 int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], double *divb_max);
 
+/* Launch configuration of a grid's kernels: blocks (of 128 threads) per
+ * launch for each kernel class, and the faces each thread of the x2/x3 flux
+ * kernels reconstructs in one strip (1..3).  hg_init picks a default;
+ * hg_autotune measures candidates on the grid's own state and keeps the
+ * fastest per kernel class: it saves the resident state, runs `steps` steps
+ * per candidate (per class: 8 block counts, and 3 strip lengths for the
+ * flux), puts the state back, and returns the chosen configuration with the
+ * device time per step before and after.  The results of a step do not
+ * depend on the configuration (M_tot's per-block partial sums aside).  No
+ * reference counterpart. */
+typedef struct hg_launch_config {
+  int32_t grid_flux, grid_flux32, grid_emf, grid_update, grid_fixup, grid_bounds;
+  int32_t strip_faces;
+  int32_t reserved;
+} hg_launch_config;
+int hg_get_launch_config(hg_handle *h, hg_launch_config *cfg);
+int hg_set_launch_config(hg_handle *h, const hg_launch_config *cfg);
+int hg_autotune(hg_handle *h, int32_t steps, hg_launch_config *best, double *ms_before, double *ms_after);
+
 /* Device time of the last hg_step call in milliseconds (CUDA events). */
 int hg_last_step_ms(hg_handle *h, double *ms);
 
