@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="torus192")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune-steps", type=int, default=3,
+                    help="steps per candidate of the launch-configuration autotuner (0: keep the defaults)")
     ap.add_argument("--mixed-steps", type=int, default=2000,
                     help="steps of the mixed-precision accuracy comparison (0: skip the mixed form)")
     return ap.parse_args()
@@ -217,7 +219,10 @@ def run_ours(args, wl, rank, world, device):
     n = wl["n"]
     e, p0 = setup(wl, device)
     # launch configuration measured on this grid's own state (restored after)
-    tuned, tune_before, tune_after = e.autotune(steps=3)
+    if args.tune_steps > 0:
+        tuned, tune_before, tune_after = e.autotune(steps=args.tune_steps)
+    else:
+        tuned, tune_before, tune_after = e.launch_config(), None, None
     zones = n[0] * n[1] * n[2]
     barrier, sync = lambda: None, lambda: None
     try:
@@ -329,6 +334,8 @@ def mixed_form(args, wl, device, e64, p0, fp64_ms):
     difference a one-ulp change of u in the initial state makes to the FP64
     run itself (how far the flow amplifies rounding)."""
     em, _ = setup(wl, device, precision=1, p_init=p0)
+    if args.tune_steps > 0:
+        em.autotune(steps=args.tune_steps)
     em.step(args.warmup)
     em.upload(p0)
     em.set_time(em.desc.t, em.desc.dx[0])

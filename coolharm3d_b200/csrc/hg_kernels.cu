@@ -1065,7 +1065,7 @@ __global__ void k_begin(DevScalars *sc)
 // t += dx[0]; dx[0] = timestep() (step_ch.c:218-223, 546-623); M_tot.
 __global__ void k_timestep(GridDev G, int nblk)
 {
-  __shared__ double red[256];
+  __shared__ double red[1024];
   double s = 0.;
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += G.blk[b];
   red[threadIdx.x] = s;
@@ -1440,7 +1440,7 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
   launch_substep(G, L, s, 0, R);
   launch_substep(G, L, s, 1, R);
   mark(R, KC_MISC, s);
-  k_timestep<<<1, 256, 0, s>>>(G, L.grid_upd);
+  k_timestep<<<1, 1024, 0, s>>>(G, L.grid_upd);
   mark(R, KC_END, s);
 }
 
