@@ -47,7 +47,8 @@ EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", 
            "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc", "hg_set_cooling_tables",
            "hg_build_geometry_ks_mks", "hg_fixup_bounds", "hg_batch_create", "hg_batch_add", "hg_batch_remove",
            "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes",
-           "hg_get_totals", "hg_get_launch_config", "hg_set_launch_config", "hg_autotune"]
+           "hg_get_totals", "hg_get_launch_config", "hg_set_launch_config", "hg_autotune",
+           "hg_write_rdump", "hg_read_rdump"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 class LaunchConfig(ctypes.Structure):
@@ -55,10 +56,10 @@ class LaunchConfig(ctypes.Structure):
     strip length of the x2/x3 flux kernels."""
     _fields_ = [("grid_flux", ctypes.c_int32), ("grid_flux32", ctypes.c_int32), ("grid_emf", ctypes.c_int32),
                 ("grid_update", ctypes.c_int32), ("grid_fixup", ctypes.c_int32), ("grid_bounds", ctypes.c_int32),
-                ("strip_faces", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("strip_faces", ctypes.c_int32), ("strip_x1", ctypes.c_int32)]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 _lib = None
@@ -107,6 +108,8 @@ def load_library(path=LIB_PATH):
     lib.hg_get_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
     lib.hg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
     lib.hg_autotune.argtypes = [P, ctypes.c_int32, ctypes.POINTER(LaunchConfig), P, P]
+    lib.hg_write_rdump.argtypes = [P, ctypes.c_char_p, ctypes.c_int32, P, ctypes.c_int32]
+    lib.hg_read_rdump.argtypes = [P, ctypes.c_char_p, P, P, P]
     lib.hg_grid_bytes.argtypes = [ctypes.POINTER(GridDesc), P]
     lib.hg_build_geometry_ks_mks.argtypes = [ctypes.POINTER(GridDesc), D, D, D, D, ctypes.c_int32, D,
                                              P, P, P, P, P, P]
@@ -284,6 +287,19 @@ class Engine:
         a, b = ctypes.c_double(), ctypes.c_double()
         _check(self.lib.hg_autotune(self.h, steps, ctypes.byref(c), ctypes.byref(a), ctypes.byref(b)), "hg_autotune")
         return c, a.value, b.value
+
+    def write_rdump(self, path, nstep=0, n_out=None, rdump_cnt=0):
+        """restart_write(): the ASCII rdump file of the resident state."""
+        no = np.ascontiguousarray(n_out if n_out is not None else np.zeros(11), np.int32)
+        _check(self.lib.hg_write_rdump(self.h, str(path).encode(), nstep, _ptr(no), rdump_cnt), "hg_write_rdump")
+
+    def read_rdump(self, path):
+        """restart_read(): load an rdump file; returns (nstep, n_out, rdump_cnt)."""
+        ns, rc = ctypes.c_int32(), ctypes.c_int32()
+        no = np.zeros(11, np.int32)
+        _check(self.lib.hg_read_rdump(self.h, str(path).encode(), ctypes.byref(ns), _ptr(no), ctypes.byref(rc)),
+               "hg_read_rdump")
+        return ns.value, no, rc.value
 
     def totals(self):
         """(U_tot[8], F_tot[3, 2, 8], max |div B|) of the last step (dump_ener)."""

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <algorithm>
 #include <new>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -23,6 +24,7 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
 void *gather_times_kernel();
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d);
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
+void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_totals(const GridDev &G, const LaunchCfg &L, cudaStream_t s, double *part, double *out);
 void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
                           double *out);
@@ -239,6 +241,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     h->L.grid_fix = grid_for(G.capacity, 2);
     h->L.grid_bnd = grid_for(faces - G.capacity, 16);
     h->L.strip_nf = 2;
+    h->L.strip_x1 = 0;
     ALLOC(G.blk, sizeof(double) * HG_BLK_CAP);
     if (cudaMallocHost((void **)&h->h_stage, (size_t)HG_XCH * HG_XCH_BYTES) != cudaSuccess) {
       cudaGetLastError();
@@ -1064,14 +1067,15 @@ static bool config_ok(const hg_launch_config *c)
   const int32_t g[6] = {c->grid_flux, c->grid_flux32, c->grid_emf, c->grid_update, c->grid_fixup, c->grid_bounds};
   for (int a = 0; a < 6; a++)
     if (g[a] < 1 || g[a] > HG_BLK_CAP) return false;
-  return c->strip_faces >= 1 && c->strip_faces <= 3;
+  return c->strip_faces >= 1 && c->strip_faces <= 3 && (c->strip_x1 == 0 || c->strip_x1 == 1);
 }
 
 extern "C" int hg_get_launch_config(hg_handle *h, hg_launch_config *c)
 {
   if (!h || !c) return HG_ERR_BADARG;
   const hg::LaunchCfg &L = h->L;
-  *c = hg_launch_config{L.grid_flux, L.grid_flux32, L.grid_emf, L.grid_upd, L.grid_fix, L.grid_bnd, L.strip_nf, 0};
+  *c = hg_launch_config{L.grid_flux, L.grid_flux32, L.grid_emf, L.grid_upd, L.grid_fix, L.grid_bnd, L.strip_nf,
+                        L.strip_x1};
   return HG_OK;
 }
 
@@ -1086,6 +1090,7 @@ extern "C" int hg_set_launch_config(hg_handle *h, const hg_launch_config *c)
   L.grid_fix = c->grid_fixup;
   L.grid_bnd = c->grid_bounds;
   L.strip_nf = c->strip_faces;
+  L.strip_x1 = c->strip_x1;
   h->graph_dirty = true;
   return HG_OK;
 }
@@ -1194,7 +1199,7 @@ extern "C" int hg_autotune(hg_handle *h, int32_t steps, hg_launch_config *best, 
     double bt = 1e300;
     hg::LaunchCfg bl = L;
     for (int a = 0; a < 8 && rc == HG_OK; a++)
-      for (int nf = 1; nf <= 3 && rc == HG_OK; nf++) {
+      for (int nf = 1; nf <= 6 && rc == HG_OK; nf++) {  // nf 4..6: strips of nf-3 faces, x1 in strips
         hg::LaunchCfg c = L;
         if (!apply(c, mults[a], nf)) continue;
         h->L = c;
@@ -1209,7 +1214,8 @@ extern "C" int hg_autotune(hg_handle *h, int32_t steps, hg_launch_config *best, 
   pick(hg::KC_FLUX, [&](hg::LaunchCfg &c, int m, int nf) {
     c.grid_flux = grid_for(faces, m);
     c.grid_flux32 = grid_for(faces, m + m / 2);
-    c.strip_nf = nf;
+    c.strip_nf = nf > 3 ? nf - 3 : nf;
+    c.strip_x1 = nf > 3;
     return true;
   });
   pick(hg::KC_EMF, [&](hg::LaunchCfg &c, int m, int nf) {
@@ -1250,5 +1256,159 @@ extern "C" int hg_autotune(hg_handle *h, int32_t steps, hg_launch_config *best, 
   if (best) hg_get_launch_config(h, best);
   if (ms_before) *ms_before = t0 / steps;
   if (ms_after) *ms_after = t1 / steps;
+  return HG_OK;
+}
+
+// ===========================================================================
+// restart_write() / restart_read() of the reference (restart.c:22-94,
+// 205-248): the ASCII rdump file of the resident state.  Header: t, N1, N2,
+// N3, GridLength[0], nstep, gam, cour, N_out[N_OUT_TYPES], rdump_cnt, dx[0]
+// ("%28.18e " for doubles, "%14d " for integers), a newline, then the
+// primitives of the physical zones in DUMP_LOOP order (i, j, k), eight
+// "%28.18e " fields and a newline per zone.  19 significant digits: every
+// double reads back exactly.  The download lands in host memory once; the
+// text of consecutive blocks of zones is formatted on HG_XCH_THREADS host
+// threads and written in order.
+// ===========================================================================
+extern "C" int hg_write_rdump(hg_handle *h, const char *path, int32_t nstep, const int32_t n_out[HG_N_OUT_TYPES],
+                              int32_t rdump_cnt)
+{
+  if (!h || !path || !n_out) return HG_ERR_BADARG;
+  if (!h->have_prims) return HG_ERR_STATE;
+  std::vector<double> p((size_t)h->ntot_ref * HG_NPR);
+  int rc = hg_download_prims(h, p.data());
+  if (rc != HG_OK) return rc;
+  hg::DevScalars sc;
+  HG_CK(copy_sync(h, &sc, h->G.sc, sizeof(sc), cudaMemcpyDeviceToHost));
+  FILE *fp = fopen(path, "wt");
+  if (!fp) return HG_ERR_BADARG;
+  fprintf(fp, "%28.18e ", sc.t);
+  fprintf(fp, "%14d ", h->d.n1);
+  fprintf(fp, "%14d ", h->d.n2);
+  fprintf(fp, "%14d ", h->d.n3);
+  fprintf(fp, "%28.18e ", h->d.grid_length[0]);
+  fprintf(fp, "%14d ", nstep);
+  fprintf(fp, "%28.18e ", h->d.gam);
+  fprintf(fp, "%28.18e ", h->d.cour);
+  for (int i = 0; i < HG_N_OUT_TYPES; i++) fprintf(fp, "%14d ", n_out[i]);
+  fprintf(fp, "%14d ", rdump_cnt);
+  fprintf(fp, "%28.18e ", sc.dt);
+  fprintf(fp, "\n");
+  const long n1 = h->d.n1, n2 = h->d.n2, n3 = h->d.n3, zones = n1 * n2 * n3;
+  const int N2T = h->NT[1], N3T = h->NT[2];
+  const long per = 1 << 15;  // zones per formatting task
+  const int nth = HG_XCH_THREADS;
+  std::vector<std::string> buf(nth);
+  bool ok = true;
+  for (long z0 = 0; z0 < zones && ok; z0 += per * nth) {
+    std::vector<std::thread> th;
+    for (int w = 0; w < nth; w++) {
+      const long a = z0 + w * per, b = std::min(zones, a + per);
+      buf[w].clear();
+      if (a >= b) continue;
+      auto job = [&, w, a, b] {
+        std::string &o = buf[w];
+        o.reserve((size_t)(b - a) * (HG_NPR * 29 + 1));
+        char line[HG_NPR * 40 + 2];
+        for (long z = a; z < b; z++) {
+          const long i = z / (n2 * n3) + HG_NG, j = (z / n3) % n2 + HG_NG, k = z % n3 + HG_NG;
+          const double *v = p.data() + ((i * N2T + j) * N3T + k) * HG_NPR;
+          int len = 0;
+          for (int l = 0; l < HG_NPR; l++) len += snprintf(line + len, sizeof(line) - len, "%28.18e ", v[l]);
+          line[len++] = '\n';
+          o.append(line, len);
+        }
+      };
+      try {
+        th.emplace_back(job);
+      } catch (...) {
+        job();
+      }
+    }
+    for (auto &t : th) t.join();
+    for (int w = 0; w < nth && ok; w++)
+      if (!buf[w].empty() && fwrite(buf[w].data(), 1, buf[w].size(), fp) != buf[w].size()) ok = false;
+  }
+  if (fclose(fp) != 0) ok = false;
+  return ok ? HG_OK : HG_ERR_BADARG;
+}
+
+extern "C" int hg_read_rdump(hg_handle *h, const char *path, int32_t *nstep, int32_t n_out[HG_N_OUT_TYPES],
+                             int32_t *rdump_cnt)
+{
+  if (!h || !path) return HG_ERR_BADARG;
+  FILE *fp = fopen(path, "rt");
+  if (!fp) return HG_ERR_BADARG;
+  double t, gl0, gam, cour, dt;
+  int n1, n2, n3, ns, rc_ = 0, no[HG_N_OUT_TYPES];
+  bool ok = fscanf(fp, "%lf %d %d %d %lf %d %lf %lf", &t, &n1, &n2, &n3, &gl0, &ns, &gam, &cour) == 8;
+  for (int i = 0; i < HG_N_OUT_TYPES && ok; i++) ok = fscanf(fp, "%d", &no[i]) == 1;
+  ok = ok && fscanf(fp, "%d %lf", &rc_, &dt) == 2;
+  if (!ok || n1 != h->d.n1 || n2 != h->d.n2 || n3 != h->d.n3) {
+    fclose(fp);
+    return HG_ERR_BADARG;
+  }
+  // the body: parse the rest of the file in parallel, one zone per line
+  const long here = ftell(fp);
+  fseek(fp, 0, SEEK_END);
+  const long end = ftell(fp);
+  fseek(fp, here, SEEK_SET);
+  std::string text((size_t)(end - here), '\0');
+  ok = fread(&text[0], 1, text.size(), fp) == text.size();
+  fclose(fp);
+  if (!ok) return HG_ERR_BADARG;
+  const long n1l = n1, n2l = n2, n3l = n3, zones = n1l * n2l * n3l;
+  std::vector<long> starts;  // offset of each zone's line
+  starts.reserve(zones + 1);
+  size_t pos = text.find('\n');
+  while (pos != std::string::npos && (long)starts.size() < zones) {
+    starts.push_back((long)pos + 1);
+    pos = text.find('\n', pos + 1);
+  }
+  if ((long)starts.size() < zones) return HG_ERR_BADARG;
+  std::vector<double> p((size_t)h->ntot_ref * HG_NPR, 0.);
+  const int N2T = h->NT[1], N3T = h->NT[2];
+  const int nth = HG_XCH_THREADS;
+  std::vector<int> bad(nth, 0);
+  std::vector<std::thread> th;
+  for (int w = 0; w < nth; w++) {
+    auto job = [&, w] {
+      for (long z = w; z < zones; z += nth) {
+        const char *c = text.c_str() + starts[z];
+        const long i = z / (n2l * n3l) + HG_NG, j = (z / n3l) % n2l + HG_NG, k = z % n3l + HG_NG;
+        double *v = p.data() + ((i * N2T + j) * N3T + k) * HG_NPR;
+        for (int l = 0; l < HG_NPR; l++) {
+          char *e;
+          v[l] = strtod(c, &e);
+          if (e == c) bad[w] = 1;
+          c = e;
+        }
+      }
+    };
+    try {
+      th.emplace_back(job);
+    } catch (...) {
+      job();
+    }
+  }
+  for (auto &t2 : th) t2.join();
+  for (int b : bad)
+    if (b) return HG_ERR_BADARG;
+  // ghost zones are filled by the boundaries, as after restart_init()
+  int rc = hg_upload_prims(h, p.data());
+  if (rc == HG_OK) rc = hg_set_time(h, t, dt);
+  if (rc == HG_OK) {
+    h->G.grid_length[0] = gl0;
+    h->d.grid_length[0] = gl0;
+    h->graph_dirty = true;
+    hg::launch_bounds_only(h->G, h->L, h->stream);
+    HG_CK(cudaGetLastError());
+    HG_CK(cudaStreamSynchronize(h->stream));
+  }
+  if (rc != HG_OK) return rc;
+  if (nstep) *nstep = ns;
+  if (n_out)
+    for (int i = 0; i < HG_N_OUT_TYPES; i++) n_out[i] = no[i];
+  if (rdump_cnt) *rdump_cnt = rc_;
   return HG_OK;
 }

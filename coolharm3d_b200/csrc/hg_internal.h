@@ -102,7 +102,8 @@ struct GridDev {
 struct LaunchCfg {
   int grid_flux, grid_emf, grid_upd, grid_fix, grid_bnd;
   int grid_flux32;  // FP32 flux kernel of the mixed form (more resident blocks)
-  int strip_nf;     // faces per thread of the strided-direction flux kernels (1..3)
+  int strip_nf;     // faces per thread of the strip flux kernels (1..3)
+  int strip_x1;     // x1 faces in strips too (else one face per thread)
 };
 #define HG_BLK_CAP 65536  // largest grid of any kernel (the per-block M_tot partials are sized for it)
 

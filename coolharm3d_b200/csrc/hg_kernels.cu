@@ -231,7 +231,11 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux(const __grid_cons
 // Face states of NF faces f0 .. f0+NF-1 along d from zones f0-3 .. f0+NF+1
 // of one variable; zones past the strip's nf faces are clamped (their
 // results are not used).  pl -> sm[bl + s], pr -> sm[br + s].
-template <bool RS, int NF>
+// X1: a strip along x1, where RESCALE_R scales each zone by its own factor
+// before the reconstruction and each face state by its face's factor after
+// it (face_prims<RS>, d = 0); along x2, x3 every value takes the
+// scale/unscale round trip of its zone i.
+template <bool RS, bool X1, int NF>
 __device__ __forceinline__ void strip_recon(const GridDev &G, const double *__restrict__ col, long st, int l, int i,
                                             int nf, double *sm, int bl, int br, int tx)
 {
@@ -241,7 +245,8 @@ __device__ __forceinline__ void strip_recon(const GridDev &G, const double *__re
   for (int c = 0; c < NF + 5; c++) {
     const int cc = c < nf + 4 ? c : nf + 4;
     double v = __ldg(col + cc * st);
-    if (RS) v = rs_roundtrip(G, v, l, i);
+    if (RS && !X1) v = rs_roundtrip(G, v, l, i);
+    if (RS && X1) v *= G.rsc[rs_type(l) * G.T[0] + i - 3 + cc];
     y[c] = v;
   }
   if (rt >= 3) {
@@ -257,6 +262,11 @@ __device__ __forceinline__ void strip_recon(const GridDev &G, const double *__re
     for (int c = 2; c <= NF + 2; c++) {
       double ln, rn;
       para_cell(y[c], I[c - 1], I[c], &ln, &rn);
+      if (RS && X1) {  // the FACE1 factors of the faces these edges belong to
+        const int t9 = (9 + rs_type(l)) * G.T[0] + i;
+        if (c - 2 < NF) rn *= G.rsc[t9 + (c - 2 < nf ? c - 2 : nf - 1)];
+        if (c - 3 >= 0) ln *= G.rsc[t9 + (c - 3 < nf ? c - 3 : nf - 1)];
+      }
       if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = rn;
       if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = ln;
     }
@@ -264,8 +274,14 @@ __device__ __forceinline__ void strip_recon(const GridDev &G, const double *__re
 #pragma unroll
     for (int c = 2; c <= NF + 2; c++) {
       const double dq = 0.5 * linear_recon(rt, y[c - 1], y[c], y[c + 1]);
-      if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = y[c] + dq;
-      if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = y[c] - dq;
+      double rn = y[c] + dq, ln = y[c] - dq;
+      if (RS && X1) {
+        const int t9 = (9 + rs_type(l)) * G.T[0] + i;
+        if (c - 2 < NF) rn *= G.rsc[t9 + (c - 2 < nf ? c - 2 : nf - 1)];
+        if (c - 3 >= 0) ln *= G.rsc[t9 + (c - 3 < nf ? c - 3 : nf - 1)];
+      }
+      if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = rn;
+      if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = ln;
     }
   }
 }
@@ -277,26 +293,36 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux_strip(const __gri
 {
   extern __shared__ double sm[];  // 16 * NF * HG_BLK doubles: the strip's face states
   const int tx = threadIdx.x;
-  const int nd = (d == 1) ? n1 : n2;
+  // x2, x3: lanes along x1, one strip per thread along d; x1: consecutive
+  // lanes take consecutive strips of the same line
+  const int nd = (d == 0) ? n0 : (d == 1) ? n1 : n2;
   const int nseg = (nd + NF - 1) / NF;
-  const int nother = (d == 1) ? n2 : n1;
-  const long total = (long)n0 * nseg * nother;
+  const long total = (long)nseg * (d == 0 ? (long)n1 * n2 : d == 1 ? (long)n0 * n2 : (long)n0 * n1);
   const long st = G.st[d];
   double vmax = 0.;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int i = lo0 + (int)(t % n0);
-    const long rest = t / n0;
-    const int seg = (int)(rest % nseg);
-    const int other = (int)(rest / nseg);
-    const int f0 = (d == 1 ? lo1 : lo2) + seg * NF;
+    int seg, i0, j0, k0;
+    if (d == 0) {
+      seg = (int)(t % nseg);
+      const long rest = t / nseg;
+      i0 = lo0 + seg * NF;
+      j0 = lo1 + (int)(rest % n1);
+      k0 = lo2 + (int)(rest / n1);
+    } else {
+      i0 = lo0 + (int)(t % n0);
+      const long rest = t / n0;
+      seg = (int)(rest % nseg);
+      const int other = (int)(rest / nseg);
+      j0 = (d == 1) ? lo1 + seg * NF : lo1 + other;
+      k0 = (d == 1) ? lo2 + other : lo2 + seg * NF;
+    }
     const int nf = min(NF, nd - seg * NF);
-    const int j0 = (d == 1) ? f0 : lo1 + other;
-    const int k0 = (d == 1) ? lo2 + other : f0;
-    const long o0 = off3(G, i, j0, k0);
+    const long o0 = off3(G, i0, j0, k0);
 #pragma unroll
     for (int l = 0; l < HG_NPR; l++)
-      strip_recon<RS, NF>(G, ph + l * G.S + o0 - 3 * st, st, l, i, nf, sm, 2 * NF * l, 2 * NF * l + NF, tx);
+      strip_recon<RS, d == 0, NF>(G, ph + l * G.S + o0 - 3 * st, st, l, i0, nf, sm, 2 * NF * l, 2 * NF * l + NF, tx);
     for (int s = 0; s < nf; s++) {
+      const int i = (d == 0) ? i0 + s : i0;
       const int j = (d == 1) ? j0 + s : j0, k = (d == 2) ? k0 + s : k0;
       double pl[HG_NPR], pr[HG_NPR];
 #pragma unroll
@@ -312,6 +338,11 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux_strip(const __gri
         Geom g;
         load_geom(G, d, i, j, g);
         ctop = face_flux(G, pl, pr, g, d, i, j, k, mult, G.F[d], o);
+      }
+      if (d == 0 && G.bc == 10) {  // fix_flux(), bounds.c:2263-2275: no mass inflow through r_in, r_out
+        double *fr = G.F[0] + RHO * G.S + o;
+        if (i == HG_NGH && *fr > 0) *fr = 0.;
+        if (i == G.NE[0] + 1 && *fr < 0) *fr = 0.;
       }
       if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
         if (ctop > vmax) vmax = ctop;
@@ -1166,7 +1197,7 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
 #define HG_STRIP(RSV, MD, DD) \
   launch_strip<RSV, MD, DD>(G, L, s, ph, lo, n, mult)
 #define HG_FLUX_D(RSV, MD) \
-  if (d == 0) HG_FLUX(RSV, MD, 0); \
+  if (d == 0) { if (G.deg[0] || !L.strip_x1) HG_FLUX(RSV, MD, 0); else HG_STRIP(RSV, MD, 0); } \
   else if (d == 1) { if (G.deg[1]) HG_FLUX(RSV, MD, 1); else HG_STRIP(RSV, MD, 1); } \
   else { if (G.deg[2]) HG_FLUX(RSV, MD, 2); else HG_STRIP(RSV, MD, 2); }
     if (G.mdim == 0) {
@@ -1434,6 +1465,12 @@ __global__ void k_gather_times(DevScalars *const *sc, int n, double *out)
 }
 
 void *gather_times_kernel() { return (void *)k_gather_times; }
+
+void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
+{
+  k_begin<<<1, 1, 0, s>>>(G.sc);
+  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0);
+}
 
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R)
 {

@@ -170,8 +170,8 @@ int hg_fixup_bounds(hg_handle *h);
 int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], double *divb_max);
 
 /* Launch configuration of a grid's kernels: blocks (of 128 threads) per
- * launch for each kernel class, and the faces each thread of the x2/x3 flux
- * kernels reconstructs in one strip (1..3).  hg_init picks a default;
+ * launch for each kernel class, the faces each thread of the strip flux
+ * kernels reconstructs in one strip (1..3), and whether x1 faces use strips.  hg_init picks a default;
  * hg_autotune measures candidates on the grid's own state and keeps the
  * fastest per kernel class: it saves the resident state, runs `steps` steps
  * per candidate (per class: 8 block counts, and 3 strip lengths for the
@@ -181,12 +181,27 @@ int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], double *divb_
  * reference counterpart. */
 typedef struct hg_launch_config {
   int32_t grid_flux, grid_flux32, grid_emf, grid_update, grid_fixup, grid_bounds;
-  int32_t strip_faces;
-  int32_t reserved;
+  int32_t strip_faces;          /* faces per thread of the strip flux kernels, 1..3 */
+  int32_t strip_x1;             /* 1: x1 faces in strips too; 0: one x1 face per thread */
 } hg_launch_config;
 int hg_get_launch_config(hg_handle *h, hg_launch_config *cfg);
 int hg_set_launch_config(hg_handle *h, const hg_launch_config *cfg);
 int hg_autotune(hg_handle *h, int32_t steps, hg_launch_config *best, double *ms_before, double *ms_after);
+
+/* restart_write() / restart_read() (restart.c:22-94, 205-248) of the
+ * resident state: the ASCII rdump file, byte for byte the layout the
+ * reference writes ("%28.18e " / "%14d " fields; header t, N1, N2, N3,
+ * GridLength[0], nstep, gam, cour, N_out[11], rdump_cnt, dx[0]; then the
+ * physical zones' primitives in DUMP_LOOP order, one zone per line).  The
+ * caller passes the driver's own counters (nstep, N_out, rdump_cnt; the
+ * reader returns them).  The reader checks N1..N3 against the grid, uploads
+ * the primitives, sets t, dx[0] and GridLength[0], and fills the ghost zones
+ * with the boundaries.  Text is formatted and parsed on host threads. */
+#define HG_N_OUT_TYPES 11
+int hg_write_rdump(hg_handle *h, const char *path, int32_t nstep, const int32_t n_out[HG_N_OUT_TYPES],
+                   int32_t rdump_cnt);
+int hg_read_rdump(hg_handle *h, const char *path, int32_t *nstep, int32_t n_out[HG_N_OUT_TYPES],
+                  int32_t *rdump_cnt);
 
 /* Device time of the last hg_step call in milliseconds (CUDA events). */
 int hg_last_step_ms(hg_handle *h, double *ms);

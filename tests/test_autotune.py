@@ -19,7 +19,8 @@ def test_autotune_keeps_state_and_results(name):
     cfg, ms0, ms1 = e.autotune(steps=2)
     np.testing.assert_array_equal(e.download(), before)
     c = cfg.as_dict()
-    assert 1 <= c["strip_faces"] <= 3 and all(v >= 1 for v in c.values())
+    assert 1 <= c["strip_faces"] <= 3 and c["strip_x1"] in (0, 1)
+    assert all(c[k] >= 1 for k in ("grid_flux", "grid_flux32", "grid_emf", "grid_update", "grid_fixup", "grid_bounds"))
     assert ms1 <= ms0 * 1.0000001
     e.set_time(f["t0"], f["dt0"])
     t_tuned = e.step(f["steps"])
@@ -29,9 +30,10 @@ def test_autotune_keeps_state_and_results(name):
     np.testing.assert_array_equal(p_tuned, ref.download())
     assert t_tuned == t_ref
     # every strip length gives the same step
-    for nf in (1, 3):
+    for nf, x1 in ((1, 1), (3, 0), (2, 1)):
         cfg2 = e.launch_config()
         cfg2.strip_faces = nf
+        cfg2.strip_x1 = x1
         cfg2.grid_flux = 7
         e.set_launch_config(cfg2)
         e.upload(f["p0"])
