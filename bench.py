@@ -69,6 +69,11 @@ WORKLOADS = {
                            "Gamma 5/3, beta 100 loop, H/R 0.1 cooling, PPM_MC+HLLE+para flux-CT, entropy fix, FP64"),
     "torus96": dict(kind="torus", n=(96, 96, 64), ref_cfg="torus", ref_block=(24, 24, 16),
                     label="Fishbone-Moncrief torus as torus192 on 96x96x64 zones"),
+    "balsara1024": dict(kind="setup", setup="balsara1", n=(1024, 1, 1), ref_cfg="balsara1", ref_block=(1024, 1, 1),
+                        label="Balsara-1 shock tube, 1024 zones, MC + HLLE + para flux-CT, CFL 0.5, FP64"),
+    "fieldloop512": dict(kind="setup", setup="field_loop", n=(512, 512, 1), ref_cfg="field_loop",
+                         ref_block=(128, 128, 1),
+                         label="advected field loop 512^2, PPM_MC + HLLE + para flux-CT, FP64"),
     "linwave256": dict(kind="linwave", n=(256, 256, 256), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
                        ref_block=(64, 64, 64),
                        label="3D periodic Minkowski linear wave 256^3, PPM_MC+HLLE+para flux-CT, FP64"),
@@ -200,6 +205,22 @@ def setup(wl, device, precision=0, p_init=None):
             p0 = p_init
             e.upload(p0)
         e.set_time(desc.t, desc.dx[0])
+        return e, p0
+    if wl["kind"] == "setup":
+        from coolharm3d_b200 import setups
+        prob = setups.balsara1(n[0], precision=precision, device=device) if wl["setup"] == "balsara1" else \
+            setups.field_loop(n, precision=precision, device=device)
+        prob.desc.grid_length[0] = 1e9  # time the step, not the approach to t_final
+        e = hg.Engine(prob.desc)
+        if p_init is None:
+            setups.start(e, prob)
+            p0 = e.download()
+        else:
+            p0 = p_init
+            e.set_geometry(prob.geom)
+            e.set_cell_data(prob.cell6)
+            e.upload(p0)
+            e.set_time(0.0, prob.desc.dx[0])
         return e, p0
     dx = [1e-5] + [1.0 / x for x in n]
     startx = [0.0] + [-3 * d for d in dx[1:]]
