@@ -25,6 +25,7 @@ void *gather_times_kernel();
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d);
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
+cudaError_t prepare_kernels();
 void launch_totals(const GridDev &G, const LaunchCfg &L, cudaStream_t s, double *part, double *out);
 void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
                           double *out);
@@ -50,7 +51,9 @@ struct hg_handle {
   double *h_stage = nullptr;  // pinned transfer chunks (HG_XCH x HG_XCH_BYTES)
   cudaEvent_t xev[HG_XCH] = {};  // DMA completion of each transfer chunk
   double *d_ref = nullptr;    // device buffer in the reference layout, when F[0] is too small
-  cudaGraph_t step_graph = nullptr;  // one hg_step(1) captured for batches (hg_batch_*)
+  cudaGraph_t step_graph = nullptr;  // one hg_step(1) captured (batches, and hg_step itself)
+  cudaGraphExec_t step_exec = nullptr;  // step_graph instantiated for hg_step
+  bool exec_stale = true;
   bool graph_dirty = true;           // the capture predates a change of the kernels' arguments
   double *d_tot = nullptr;           // hg_get_totals: per-block partials and the result
   int batch_refs = 0;                // batches this grid belongs to
@@ -191,7 +194,9 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     if ((rc = dev_alloc(h, &q_, (bytes))) != HG_OK) goto fail; \
     ptr = (decltype(ptr))q_;                                  \
   } while (0)
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (hg::prepare_kernels() != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
     delete h;
     return HG_ERR_CUDA;
   }
@@ -286,6 +291,7 @@ extern "C" void hg_destroy(hg_handle *h)
   for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_stage) cudaFreeHost(h->h_stage);
+  if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
   if (h->step_graph) cudaGraphDestroy(h->step_graph);
   for (int x = 0; x < HG_XCH; x++)
     if (h->xev[x]) cudaEventDestroy(h->xev[x]);
@@ -595,6 +601,23 @@ extern "C" int hg_set_time(hg_handle *h, double t, double dt)
   return HG_OK;
 }
 
+static int capture_step(hg_handle *h);
+
+static int step_exec_ready(hg_handle *h)
+{
+  const bool recaptured = !h->step_graph || h->graph_dirty;
+  int rc = capture_step(h);
+  if (rc != HG_OK) return rc;
+  if (h->step_exec && !recaptured && !h->exec_stale) return HG_OK;
+  if (h->step_exec) {
+    cudaGraphExecDestroy(h->step_exec);
+    h->step_exec = nullptr;
+  }
+  HG_CK(cudaGraphInstantiate(&h->step_exec, h->step_graph, 0));
+  h->exec_stale = false;
+  return HG_OK;
+}
+
 extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
 {
   if (!h || nsteps < 0) return HG_ERR_BADARG;
@@ -616,8 +639,18 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
     rec.cap = (int)h->pev.size();
     R = &rec;
   }
+  // Without per-kernel events the step runs as one CUDA graph launch (the
+  // same kernels with the same arguments, captured once), which takes the
+  // host's launch cost of small grids off the step.
+  if (!R && nsteps > 0) {
+    int rc = step_exec_ready(h);
+    if (rc != HG_OK) return rc;
+  }
   HG_CK(cudaEventRecord(h->ev0, h->stream));
-  for (int s = 0; s < nsteps; s++) hg::launch_step(h->G, h->L, h->stream, R);
+  for (int s = 0; s < nsteps; s++) {
+    if (R) hg::launch_step(h->G, h->L, h->stream, R);
+    else HG_CK(cudaGraphLaunch(h->step_exec, h->stream));
+  }
   HG_CK(cudaGetLastError());
   HG_CK(cudaEventRecord(h->ev1, h->stream));
   HG_CK(cudaEventSynchronize(h->ev1));
@@ -852,6 +885,7 @@ static int capture_step(hg_handle *h)
   HG_CK(cudaGetLastError());
   h->step_graph = g;
   h->graph_dirty = false;
+  h->exec_stale = true;
   return HG_OK;
 }
 

@@ -1149,12 +1149,36 @@ static void launch_strip_nf(const GridDev &G, const LaunchCfg &L, cudaStream_t s
                             const int *n, unsigned int mult)
 {
   const size_t smem = sizeof(double) * 16 * NF * HG_BLK;
-  static bool ready = false;
-  if (!ready) {
-    cudaFuncSetAttribute(k_flux_strip<RS, MDIM, d, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    ready = true;
-  }
   k_flux_strip<RS, MDIM, d, NF><<<L.grid_flux, HG_BLK, smem, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult);
+}
+
+template <bool RS, int MDIM, int d, int NF>
+static cudaError_t strip_attr()
+{
+  return cudaFuncSetAttribute(k_flux_strip<RS, MDIM, d, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sizeof(double) * 16 * NF * HG_BLK));
+}
+
+template <bool RS, int MDIM>
+static cudaError_t strip_attrs_rm()
+{
+  cudaError_t e = cudaSuccess;
+  const cudaError_t r[9] = {strip_attr<RS, MDIM, 0, 1>(), strip_attr<RS, MDIM, 0, 2>(), strip_attr<RS, MDIM, 0, 3>(),
+                            strip_attr<RS, MDIM, 1, 1>(), strip_attr<RS, MDIM, 1, 2>(), strip_attr<RS, MDIM, 1, 3>(),
+                            strip_attr<RS, MDIM, 2, 1>(), strip_attr<RS, MDIM, 2, 2>(), strip_attr<RS, MDIM, 2, 3>()};
+  for (cudaError_t x : r)
+    if (x != cudaSuccess) e = x;
+  return e;
+}
+
+// Kernel attributes that must be set before a launch (the strip kernels'
+// shared memory above the default limit), once per device, outside any
+// stream capture: called by hg_init.
+cudaError_t prepare_kernels()
+{
+  cudaError_t e = strip_attrs_rm<false, 0>();
+  const cudaError_t e1 = strip_attrs_rm<true, 0>(), e2 = strip_attrs_rm<false, 2>(), e3 = strip_attrs_rm<true, 2>();
+  return e != cudaSuccess ? e : e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3;
 }
 
 // strips of L.strip_nf faces (1, 2 or 3: a launch-configuration choice)
