@@ -1136,7 +1136,8 @@ static inline void mark(EventRec *r, int cls, cudaStream_t s)
   r->n++;
 }
 
-void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const int *lo, const int *n, unsigned int mult);
+void launch_flux_f32(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d, const int *lo, const int *n,
+                     unsigned int mult);
 void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
 
 // k_flux_strip keeps 16 * NF face states per thread in dynamic shared memory
@@ -1214,7 +1215,7 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
     }
     mark(R, KC_FLUX, s);
     if (G.prec == HG_PREC_MIXED) {
-      launch_flux_f32(G, L.grid_flux32, s, d, lo, n, mult);  // reads G.p32, filled from ph
+      launch_flux_f32(G, L, s, d, lo, n, mult);  // reads G.p32, filled from ph
       return;
     }
 #define HG_FLUX(RSV, MD, DD) k_flux<RSV, MD, DD><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)

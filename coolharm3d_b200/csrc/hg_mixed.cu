@@ -182,17 +182,23 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_f32(const __gri
 // Strips of NF consecutive faces along a strided direction (x2, x3), lanes
 // along x1: each zone's PPM edges are formed once per strip (the FP64
 // k_flux_strip's scheme); the strip's face states wait in shared memory.
-#ifndef HG_STRIP32_NF
-#define HG_STRIP32_NF 3
-#endif
 
-template <int NF>
-__device__ __forceinline__ void strip_recon_f32(int rt, const float *__restrict__ col, long st, int nf, float *sm,
-                                                int bl, int br, int tx)
+// X1 with RESCALE_R: zones scaled by their factors before, face states by
+// their faces' factors after the reconstruction (FP32 copies of the tables).
+template <bool RS, bool X1, int NF>
+__device__ __forceinline__ void strip_recon_f32(const GridDev &G, const float *__restrict__ col, long st, int l, int i,
+                                                int nf, float *sm, int bl, int br, int tx)
 {
+  const int rt = G.recon;
   float y[NF + 5];
 #pragma unroll
-  for (int c = 0; c < NF + 5; c++) y[c] = __ldg(col + (c < nf + 4 ? c : nf + 4) * st);
+  for (int c = 0; c < NF + 5; c++) {
+    const int cc = c < nf + 4 ? c : nf + 4;
+    float v = __ldg(col + cc * st);
+    if (RS && X1) v *= __ldg(G.rsc32 + rs_type(l) * G.T[0] + i - 3 + cc);
+    y[c] = v;
+  }
+  float rnv[NF + 3], lnv[NF + 3];
   if (rt >= 3) {
     float q[NF + 4];
 #pragma unroll
@@ -201,19 +207,25 @@ __device__ __forceinline__ void strip_recon_f32(int rt, const float *__restrict_
 #pragma unroll
     for (int c = 1; c <= NF + 2; c++) I[c] = 0.5f * (y[c + 1] + y[c]) - float(HG_PPM_FACTOR) * (q[c + 1] - q[c]);
 #pragma unroll
-    for (int c = 2; c <= NF + 2; c++) {
-      float ln, rn;
-      para_cell(y[c], I[c - 1], I[c], &ln, &rn);
-      if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = rn;
-      if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = ln;
-    }
+    for (int c = 2; c <= NF + 2; c++) para_cell(y[c], I[c - 1], I[c], &lnv[c], &rnv[c]);
   } else {
 #pragma unroll
     for (int c = 2; c <= NF + 2; c++) {
       const float dq = 0.5f * linear_recon(rt, y[c - 1], y[c], y[c + 1]);
-      if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = y[c] + dq;
-      if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = y[c] - dq;
+      rnv[c] = y[c] + dq;
+      lnv[c] = y[c] - dq;
     }
+  }
+#pragma unroll
+  for (int c = 2; c <= NF + 2; c++) {
+    float rn = rnv[c], ln = lnv[c];
+    if (RS && X1) {
+      const float *f = G.rsc32 + (9 + rs_type(l)) * G.T[0] + i;
+      if (c - 2 < NF) rn *= __ldg(f + (c - 2 < nf ? c - 2 : nf - 1));
+      if (c - 3 >= 0) ln *= __ldg(f + (c - 3 < nf ? c - 3 : nf - 1));
+    }
+    if (c - 2 < NF) sm[(bl + c - 2) * HG_BLK + tx] = rn;
+    if (c - 3 >= 0) sm[(br + c - 3) * HG_BLK + tx] = ln;
   }
 }
 
@@ -257,33 +269,42 @@ __device__ __forceinline__ float face_flux_f32(const GridDev &G, const float *pl
   return ctop;
 }
 
-template <int MDIM, int d, int NF>
+template <bool RS, int MDIM, int d, int NF>
 __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const __grid_constant__ GridDev G, int lo0,
                                                                           int lo1, int lo2, int n0, int n1, int n2,
                                                                           unsigned int mult)
 {
   __shared__ float sm[16 * NF * HG_BLK];
   const int tx = threadIdx.x;
-  const int nd = (d == 1) ? n1 : n2;
+  const int nd = (d == 0) ? n0 : (d == 1) ? n1 : n2;
   const int nseg = (nd + NF - 1) / NF;
-  const int nother = (d == 1) ? n2 : n1;
-  const long total = (long)n0 * nseg * nother;
+  const long total = (long)nseg * (d == 0 ? (long)n1 * n2 : d == 1 ? (long)n0 * n2 : (long)n0 * n1);
   const long st = G.st[d];
   double vmax = 0.;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int i = lo0 + (int)(t % n0);
-    const long rest = t / n0;
-    const int seg = (int)(rest % nseg);
-    const int other = (int)(rest / nseg);
-    const int f0 = (d == 1 ? lo1 : lo2) + seg * NF;
+    int seg, i0, j0, k0;
+    if (d == 0) {  // consecutive lanes on consecutive strips of a line
+      seg = (int)(t % nseg);
+      const long rest = t / nseg;
+      i0 = lo0 + seg * NF;
+      j0 = lo1 + (int)(rest % n1);
+      k0 = lo2 + (int)(rest / n1);
+    } else {  // lanes along x1
+      i0 = lo0 + (int)(t % n0);
+      const long rest = t / n0;
+      seg = (int)(rest % nseg);
+      const int other = (int)(rest / nseg);
+      j0 = (d == 1) ? lo1 + seg * NF : lo1 + other;
+      k0 = (d == 1) ? lo2 + other : lo2 + seg * NF;
+    }
     const int nf = min(NF, nd - seg * NF);
-    const int j0 = (d == 1) ? f0 : lo1 + other;
-    const int k0 = (d == 1) ? lo2 + other : f0;
-    const long o0 = off3(G, i, j0, k0);
+    const long o0 = off3(G, i0, j0, k0);
 #pragma unroll
     for (int l = 0; l < HG_NPR; l++)
-      strip_recon_f32<NF>(G.recon, G.p32 + l * G.S + o0 - 3 * st, st, nf, sm, 2 * NF * l, 2 * NF * l + NF, tx);
+      strip_recon_f32<RS, d == 0, NF>(G, G.p32 + l * G.S + o0 - 3 * st, st, l, i0, nf, sm, 2 * NF * l,
+                                      2 * NF * l + NF, tx);
     for (int s = 0; s < nf; s++) {
+      const int i = (d == 0) ? i0 + s : i0;
       const int j = (d == 1) ? j0 + s : j0, k = (d == 2) ? k0 + s : k0;
       float pl[HG_NPR], pr[HG_NPR];
 #pragma unroll
@@ -291,7 +312,13 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const
         pl[l] = sm[(2 * NF * l + s) * HG_BLK + tx];
         pr[l] = sm[(2 * NF * l + NF + s) * HG_BLK + tx];
       }
-      const float ctop = face_flux_f32<MDIM, d>(G, pl, pr, i, j, k, mult, o0 + s * st);
+      const long o = o0 + s * st;
+      const float ctop = face_flux_f32<MDIM, d>(G, pl, pr, i, j, k, mult, o);
+      if (d == 0 && G.bc == 10) {  // fix_flux(), bounds.c:2263-2275
+        double *fr = G.F[0] + RHO * G.S + o;
+        if (i == HG_NGH && *fr > 0) *fr = 0.;
+        if (i == G.NE[0] + 1 && *fr < 0) *fr = 0.;
+      }
       if (i >= HG_NGH && i <= G.NE[0] && j >= HG_NGH && j <= G.NE[1] && k >= HG_NGH && k <= G.NE[2])
         if ((double)ctop > vmax) vmax = (double)ctop;
     }
@@ -299,16 +326,28 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const
   block_max_atomic(vmax, &G.sc->maxs[d + 1]);
 }
 
-void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const int *lo, const int *n, unsigned int mult)
+template <bool RS, int MDIM, int d>
+static void launch_strip32(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const int *lo, const int *n,
+                           unsigned int mult)
 {
+#define HG_S32N(NF) \
+  k_flux_strip_f32<RS, MDIM, d, NF><<<L.grid_flux32, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
+  if (L.strip_nf <= 1) HG_S32N(1);
+  else if (L.strip_nf == 2) HG_S32N(2);
+  else HG_S32N(3);
+#undef HG_S32N
+}
+
+void launch_flux_f32(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d, const int *lo, const int *n,
+                     unsigned int mult)
+{
+  const int grid = L.grid_flux32;
 #define HG_F32(RSV, MD, DD) \
   k_flux_f32<RSV, MD, DD><<<grid, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
-#define HG_S32(MD, DD) \
-  k_flux_strip_f32<MD, DD, HG_STRIP32_NF><<<grid, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
 #define HG_F32_D(RSV, MD) \
-  if (d == 0) HG_F32(RSV, MD, 0); \
-  else if (d == 1) { if (G.deg[1]) HG_F32(RSV, MD, 1); else HG_S32(MD, 1); } \
-  else { if (G.deg[2]) HG_F32(RSV, MD, 2); else HG_S32(MD, 2); }
+  if (d == 0) { if (G.deg[0] || !L.strip_x1) HG_F32(RSV, MD, 0); else launch_strip32<RSV, MD, 0>(G, L, s, lo, n, mult); } \
+  else if (d == 1) { if (G.deg[1]) HG_F32(RSV, MD, 1); else launch_strip32<RSV, MD, 1>(G, L, s, lo, n, mult); } \
+  else { if (G.deg[2]) HG_F32(RSV, MD, 2); else launch_strip32<RSV, MD, 2>(G, L, s, lo, n, mult); }
   if (G.mdim == 0) {
     if (G.rescale) { HG_F32_D(true, 0) }
     else { HG_F32_D(false, 0) }
@@ -317,7 +356,6 @@ void launch_flux_f32(const GridDev &G, int grid, cudaStream_t s, int d, const in
     else { HG_F32_D(false, 2) }
   }
 #undef HG_F32_D
-#undef HG_S32
 #undef HG_F32
 }
 

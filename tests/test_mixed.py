@@ -105,3 +105,22 @@ def test_divb_stays_at_roundoff(precision):
     print("precision", precision, "max |div B| / scale", rel)
     assert rel < 1e-12
     e.close()
+
+
+def test_mixed_launch_configurations_agree():
+    """The FP32 flux kernels with x1 strips and other strip lengths give the
+    per-face FP32 result up to FP32 rounding (the compiler may contract
+    multiply-adds differently in each kernel)."""
+    f = fixtures.load("torus_24x16x8_s3")
+    runs = []
+    for x1, nf in ((0, 2), (1, 1), (1, 3)):
+        e = fixture_engine(f, hg.PREC_MIXED)
+        c = e.launch_config()
+        c.strip_x1, c.strip_faces = x1, nf
+        e.set_launch_config(c)
+        e.step(3)
+        runs.append(e.download())
+        e.close()
+    for p in runs[1:]:
+        err = l1_rel(p, runs[0])
+        assert max(err.values()) < 1e-5, err
