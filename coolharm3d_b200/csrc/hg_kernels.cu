@@ -406,14 +406,20 @@ __global__ void __launch_bounds__(HG_BLK) k_emf(GridDev G, int lo0, int lo1, int
 // ---------------------------------------------------------------------------
 // source(), phys.c:121-187 (cooling off): T^mu_kappa Gamma^kappa_nu mu for
 // METRIC_DIM 2 (U1, U2 only), times sqrt(-g).  Returns 1 on a gamma failure.
-__device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, const Geom &g, int i, int j, double *dU)
+// With PRE the state of ph is given (qpre, and badpre the result of its
+// gamma_calc): the predictor's sources are evaluated at p_i, whose state the
+// conserved variables already needed.
+template <bool PRE>
+__device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, const Geom &g, int i, int j, double *dU,
+                                            const State &qpre, int badpre)
 {
 #pragma unroll
   for (int l = 0; l < HG_NPR; l++) dU[l] = 0.;
   int bad = 0;
   State q;
+  if (PRE) q = qpre;
   if (G.mdim > 0) {
-    bad = get_state(ph, g, G.gam, q);
+    bad = PRE ? badpre : get_state(ph, g, G.gam, q);
     double mhd[4][4];
     mhd_row(q, 0, mhd[0]);
     mhd_row(q, 1, mhd[1]);
@@ -430,7 +436,7 @@ __device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, 
       }
   }
   if (G.cooling == 1) {  // phys.c:162-172, source_cooling_func phys.c:541-582
-    if (G.mdim == 0) bad = get_state(ph, g, G.gam, q);
+    if (G.mdim == 0) bad = PRE ? badpre : get_state(ph, g, G.gam, q);
     const int bound = ((q.ucov[0] * (q.p + ph[UU] + ph[RHO] + q.bsq)) > (-ph[RHO])) ? 1 : 0;
     double f_cool = 0.;
     if (bound) {  // cooling_func_hr_disk, phys.c:779-783 (s_norm 1, q_exp 1/2)
@@ -523,13 +529,12 @@ __global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __gr
       const double v = p[l * S + o];
       pi[l] = RS ? rs_roundtrip(G, v, l, i) : v;
     }
-    {  // U(p_i) at the start of the step (U_gf[0])
-      State q;
-      if (get_state(pi, g, G.gam, q) && sub == 0) book(G, NF_GAMMA_CALC, i, j, k);
-      primtoflux(pi, q, 0, g, U);
-    }
+    State q;  // U(p_i) at the start of the step (U_gf[0])
+    const int bad_i = get_state(pi, g, G.gam, q);
+    if (bad_i && sub == 0) book(G, NF_GAMMA_CALC, i, j, k);
+    primtoflux(pi, q, 0, g, U);
     if (sub == 0) {
-      if (source_terms(G, pi, g, i, j, dU)) book(G, NF_GAMMA_CALC, i, j, k);
+      if (source_terms<true>(G, pi, g, i, j, dU, q, bad_i)) book(G, NF_GAMMA_CALC, i, j, k);
     } else {
       double phv[HG_NPR];
 #pragma unroll
@@ -537,7 +542,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __gr
         const double v = p_h[l * S + o];
         phv[l] = RS ? rs_roundtrip(G, v, l, i) : v;
       }
-      if (source_terms(G, phv, g, i, j, dU)) book(G, NF_GAMMA_CALC, i, j, k);
+      if (source_terms<false>(G, phv, g, i, j, dU, q, 0)) book(G, NF_GAMMA_CALC, i, j, k);
     }
     update_zone(G, i, j, k, Dt, dU, U);
     msum += U[0];
