@@ -213,6 +213,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     ALLOC(G.sc, sizeof(hg::DevScalars));
     ALLOC(G.q_idx, sizeof(unsigned long long) * G.capacity);
     ALLOC(G.q_U, sizeof(double) * HG_NPR * G.capacity);
+    if (G.use_ee) ALLOC(G.q_F, sizeof(double) * 6 * G.capacity);
     ALLOC(G.fl_idx, sizeof(unsigned long long) * G.capacity);
     if (G.mdim == 2) {
       G.gS = (long)HG_NPOS * G.T[0] * G.T[1];
@@ -1057,6 +1058,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   b += 8ull * S * 3 + 8ull * S + 4ull * S;    // emf[3], p_gamma, pflag
   b += 4ull * S * HG_NF + 8ull * S * 2;       // nfail, floors
   b += sizeof(hg::DevScalars) + 8ull * cap * (2 + HG_NPR);  // scalars, queue, flagged list
+  if (d->use_entropy_eq) b += 8ull * 6 * cap;                 // entropy face fluxes of the queue
   if (d->metric_dim == 2) b += 8ull * 42 * gS + 8ull * 64 * T[0] * T[1];
   if (d->rescale_r) b += 8ull * 12 * T[0];
   if (d->cooling) b += 8ull * 2 * T[0];

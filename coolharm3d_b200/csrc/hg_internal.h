@@ -73,6 +73,7 @@ struct GridDev {
   // 2) and FP32 RESCALE_R factors (12 planes of T0)
   float *p32, *geomF, *rsc32;
   double *Uc;                // conserved variables after the update (8 planes of S)
+  double *q_F;               // entropy face fluxes of the queued zones (6 per queue slot)
   double gam, cour;
   double dx[4], invdx[4];
   double startx[4], grid_length[4];

@@ -658,8 +658,24 @@ __device__ __noinline__ double ee_face_flux(const GridDev &G, const double *p_h,
   return 0.5 * (Fl + Fr - ctop * (Ur - Ul));
 }
 
+// The six entropy face fluxes of every queued zone, one (zone, face) per
+// thread, ahead of k_fallback: q_F[6 e + f], f = 0..2 the lower faces of
+// x1..x3, 3..5 the upper ones.
 template <bool RS>
-__device__ __noinline__ int fixup_entropy_eq(const GridDev &G, const double *p_h, int i, int j, int k,
+__global__ void __launch_bounds__(HG_BLK) k_ee_faces(GridDev G, const double *__restrict__ p_h)
+{
+  const long n = 6L * min(G.sc->q_count, (int)G.capacity);
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const long e = t / 6;
+    const int f = (int)(t % 6), d = f % 3, up = f / 3;
+    int i, j, k;
+    unpack_ijk(G.q_idx[e], i, j, k);
+    G.q_F[t] = ee_face_flux<RS>(G, p_h, d, i + (up && d == 0), j + (up && d == 1), k + (up && d == 2));
+  }
+}
+
+template <bool RS>
+__device__ __noinline__ int fixup_entropy_eq(const GridDev &G, long e, int i, int j, int k,
                                              const double *prim_old, double *prim, const Geom &geom,
                                              const double *Un, double Dt, double *gamma_out)
 {
@@ -669,8 +685,10 @@ __device__ __noinline__ int fixup_entropy_eq(const GridDev &G, const double *p_h
   gamma_calc(prim_old, geom, &gamma);
   const double S_old = geom.g * (gam - 1.) * prim_old[UU] * gamma / (geom.alpha * pow(prim_old[RHO], (gam - 1.)));
   double Fm[3], Fp[3];
-  for (int d = 0; d < 3; d++) Fm[d] = ee_face_flux<RS>(G, p_h, d, i, j, k);
-  for (int d = 0; d < 3; d++) Fp[d] = ee_face_flux<RS>(G, p_h, d, i + (d == 0), j + (d == 1), k + (d == 2));
+  for (int d = 0; d < 3; d++) {
+    Fm[d] = G.q_F[6 * e + d];
+    Fp[d] = G.q_F[6 * e + 3 + d];
+  }
   const double Snew = S_old + Dt * (-(Fp[0] - Fm[0]) * G.invdx[1] - (Fp[1] - Fm[1]) * G.invdx[2] -
                                     (Fp[2] - Fm[2]) * G.invdx[3]);
   int ret = utoprim_1d_ee(Un, Snew, geom, gam, prim, &gamma);
@@ -746,7 +764,7 @@ __global__ void __launch_bounds__(HG_BLK) k_fallback(GridDev G, int sub, double 
         book(G, NF_UTOPRIM, i, j, k);
       }
       for (int l = 0; l < B1; l++) pf[l] = pg[l];
-      const int ret_ee = fixup_entropy_eq<RS>(G, p_h, i, j, k, pold, pf, g, U, Dt, &gamma);
+      const int ret_ee = fixup_entropy_eq<RS>(G, e, i, j, k, pold, pf, g, U, Dt, &gamma);
       if (ret_ee) {
         if (ret) {
           book(G, NF_UTOPRIM_EE, i, j, k);
@@ -1273,6 +1291,10 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
   }
 #undef HG_UPD
   mark(R, KC_FALLBACK, s);
+  if (G.use_ee) {
+    if (G.rescale) k_ee_faces<true><<<L.grid_fix * 6, HG_BLK, 0, s>>>(G, ph);
+    else k_ee_faces<false><<<L.grid_fix * 6, HG_BLK, 0, s>>>(G, ph);
+  }
   if (G.rescale) k_fallback<true><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
   else k_fallback<false><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
   mark(R, KC_BOUNDS, s);
