@@ -115,6 +115,122 @@ def linear_wave(n, amp=1.0e-4, cour=0.4, precision=PREC_FP64, device=0):
     return _problem("linear_wave", desc, p, tf)
 
 
+def _minkowski_u_f(P, gam):
+    """HARM's conserved variables and its three directional fluxes of ideal
+    MHD in Minkowski space for one primitive state P = (rho, u, u~1..3,
+    B1..3): ucon_calc / bcon_calc (phys.c:216, 75) with alpha 1, beta 0;
+    mhd_calc (phys.c:93) T^mu_nu = w u^mu u_nu + p_tot delta - b^mu b_nu;
+    primtoflux (phys.c:28): rho u^mu, T^mu_t + rho u^mu, T^mu_j,
+    b^j u^mu - b^mu u^j (B^j itself for mu = t).  Works on complex P, for
+    complex-step derivatives."""
+    rho, u, v1, v2, v3, B1, B2, B3 = P
+    ut = np.sqrt(1.0 + v1 * v1 + v2 * v2 + v3 * v3)
+    ucon = [ut, v1, v2, v3]
+    bt = B1 * v1 + B2 * v2 + B3 * v3
+    bcon = [bt] + [(Bj + bt * ucon[j + 1]) / ut for j, Bj in enumerate((B1, B2, B3))]
+    sgn = (-1.0, 1.0, 1.0, 1.0)
+    ucov = [sgn[m] * ucon[m] for m in range(4)]
+    bcov = [sgn[m] * bcon[m] for m in range(4)]
+    bsq = sum(bcon[m] * bcov[m] for m in range(4))
+    pg = (gam - 1.0) * u
+    w, ptot = rho + u + pg + bsq, pg + 0.5 * bsq
+
+    def row(mu):
+        T = [w * ucon[mu] * ucov[nu] + (ptot if mu == nu else 0.0) - bcon[mu] * bcov[nu] for nu in range(4)]
+        out = [rho * ucon[mu], T[0] + rho * ucon[mu], T[1], T[2], T[3]]
+        out += [B1, B2, B3] if mu == 0 else [bcon[j] * ucon[mu] - bcon[mu] * ucon[j] for j in (1, 2, 3)]
+        return np.array(out)
+
+    return row(0), [row(1), row(2), row(3)]
+
+
+def rmhd_modes(rho, pgas, gam, B, nhat):
+    """Linear eigenmodes of relativistic ideal MHD about the static state
+    (rho, p, v = 0, B) for plane waves along nhat: the eigenvalues lambda
+    (wave speeds, ascending: fast-, Alfven-, slow-, entropy, slow+, Alfven+,
+    fast+) and primitive right eigenvectors R (8 x 7, columns in the same
+    order) of  n_d dF^d/dP R = lambda dU/dP R  with dB.nhat = 0.  The
+    Jacobians are complex-step derivatives of _minkowski_u_f; the perturbed
+    field is restricted to the plane normal to nhat and the equations
+    projected on it, which drops the zero-speed divergence mode.  The
+    reference's closed forms (eigs(), init.linearwave.c:166-240, for
+    B = (Bx, 0, 0) along k = 2 pi (1, 1, 0)) are special cases."""
+    nhat = np.asarray(nhat, float) / np.linalg.norm(nhat)
+    P = np.array([rho, pgas / (gam - 1.0), 0.0, 0.0, 0.0, *B], float)
+    h = 1.0e-30
+    dU, dF = np.zeros((8, 8)), np.zeros((8, 8))
+    for c in range(8):
+        Pc = P.astype(complex)
+        Pc[c] += 1j * h
+        U, F = _minkowski_u_f(Pc, gam)
+        dU[:, c] = U.imag / h
+        dF[:, c] = sum(nhat[d] * F[d].imag for d in range(3)) / h
+    a = np.array([1.0, 0.0, 0.0]) if abs(nhat[0]) < 0.9 else np.array([0.0, 1.0, 0.0])
+    e1 = a - nhat * np.dot(a, nhat)
+    e1 /= np.linalg.norm(e1)
+    e2 = np.cross(nhat, e1)
+    Q = np.zeros((8, 7))
+    Q[:5, :5] = np.eye(5)
+    Q[5:, 5], Q[5:, 6] = e1, e2
+    A = np.linalg.solve(Q.T @ dU @ Q, Q.T @ dF @ Q)
+    lam, V = np.linalg.eig(A)
+    if np.abs(lam.imag).max() > 1e-12 or np.abs(V.imag).max() > 1e-12:
+        raise ValueError("complex eigenmodes: the background state is not hyperbolic")
+    o = np.argsort(lam.real)
+    return lam.real[o], Q @ V.real[:, o]
+
+
+MODES = {"fast": 6, "alfven": 5, "slow": 4}
+
+
+def eigenmode(mode, rho, pgas, gam, B, nhat):
+    """One right-moving mode ('fast', 'alfven' or 'slow') of rmhd_modes:
+    (dp, lambda), dp scaled so that its largest component is +1.  Raises
+    ValueError if the mode's speed is degenerate with a neighbour's (field
+    along nhat or normal to it), where the eigenvector is not unique."""
+    lam, R = rmhd_modes(rho, pgas, gam, B, nhat)
+    m = MODES[mode]
+    gap = min(abs(lam[m] - lam[m - 1]), abs(lam[m + 1] - lam[m]) if m < 6 else np.inf)
+    if gap < 1e-8:
+        raise ValueError("%s mode is degenerate for this field direction" % mode)
+    dp = R[:, m] / R[np.argmax(np.abs(R[:, m])), m]
+    dp[np.abs(dp) < 1e-14] = 0.0
+    return dp, float(lam[m])
+
+
+def linear_wave_3d(n, mode="fast", amp=1.0e-6, rho=1.0, pgas=1.0, gam=4.0 / 3.0, B=(1.0, 1.5, 0.0), kvec=(1, 1, 1),
+                   cour=0.4, recon=RECON_PPM_MC, precision=PREC_FP64, device=0):
+    """Periodic linear wave of one exact RMHD eigenmode on the unit box:
+    p = p0 + amp dp cos(k.x), k = 2 pi kvec (integers, so the box holds
+    whole wavelengths), with (dp, lambda) from eigenmode along kvec; one
+    period is t_f = 2 pi / (|k| lambda), after which the exact solution is
+    the initial state again.  The default is the fast mode of rho 1, p 1,
+    B (1, 1.5, 0), Gamma 4/3 along the grid diagonal at amplitude 1e-6;
+    PPM_MC (or `recon`) + HLLE + para flux-CT like the reference's
+    linear-wave test (init.linearwave.c).  With n3 = 1, kvec must have no x3
+    component."""
+    n = tuple(int(x) for x in n)
+    kvec = np.asarray(kvec, float)
+    if n[2] == 1 and kvec[2] != 0:
+        raise ValueError("a grid with one zone in x3 cannot hold a wave with k3 != 0")
+    dp, lam = eigenmode(mode, rho, pgas, gam, B, kvec)
+    k = 2.0 * math.pi * kvec
+    tf = 2.0 * math.pi / (np.linalg.norm(k) * lam)
+    dx = [1.0e-5] + [1.0 / x for x in n]
+    startx = [0.0] + [0.0 - NG * dx[a] for a in (1, 2, 3)]
+    desc = make_desc(n, gam, cour, dx, startx, [tf, 1.0, 1.0, 1.0], recon=recon, flux=FLUX_HLLE, ct_para=1,
+                     bc=BC_CARTESIAN_PERIODIC, metric_dim=0, use_ee=1, precision=precision, device=device)
+    shp = ref_shape(n)
+    x1, x2, x3 = (_centres(desc, a) for a in (1, 2, 3))
+    eph = np.cos(k[0] * x1[:, None, None] + k[1] * x2[None, :, None] + k[2] * x3[None, None, :])
+    base = np.array([rho, pgas / (gam - 1.0), 0.0, 0.0, 0.0, *B])
+    p = np.zeros(shp + (8,))
+    sl = tuple(slice(NG, NG + x) for x in n)
+    for l in range(8):
+        p[sl + (l,)] = (base[l] + dp[l] * amp * eph)[sl]
+    return _problem("linear_wave_3d_" + mode, desc, p, tf)
+
+
 def field_loop(n, v0=0.5, loop_radius=0.3, az0=1.0e-3, cour=0.4, precision=PREC_FP64, device=0):
     """Advected magnetic field loop (init.field_loop.c; Gardiner & Stone 2005)
     on [-3, 3]^2, periodic, Gamma 5/3, rho 1, p 3, v = (v0, v0/2, 0), to
