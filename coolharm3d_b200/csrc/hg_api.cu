@@ -246,8 +246,8 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     h->L.grid_upd = grid_for(G.capacity, 128);
     h->L.grid_fix = grid_for(G.capacity, 2);
     h->L.grid_bnd = grid_for(faces - G.capacity, 16);
-    h->L.strip_nf = 2;
-    h->L.strip_x1 = 0;
+    h->L.strip_nf = 2;  // 2-face strips in all three directions (with these
+    h->L.strip_x1 = 1;  // block counts, the torus's fastest)
     ALLOC(G.blk, sizeof(double) * HG_BLK_CAP);
     if (cudaMallocHost((void **)&h->h_stage, (size_t)HG_XCH * HG_XCH_BYTES) != cudaSuccess) {
       cudaGetLastError();
