@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux_strip(const __gri
     }
     const int nf = min(NF, nd - seg * NF);
     const long o0 = off3(G, i0, j0, k0);
-#pragma unroll
+#pragma unroll 1  // one copy of the reconstruction code: the kernel fits the instruction cache
     for (int l = 0; l < HG_NPR; l++)
       strip_recon<RS, d == 0, NF>(G, ph + l * G.S + o0 - 3 * st, st, l, i0, nf, sm, 2 * NF * l, 2 * NF * l + NF, tx);
     for (int s = 0; s < nf; s++) {

@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const
     }
     const int nf = min(NF, nd - seg * NF);
     const long o0 = off3(G, i0, j0, k0);
-#pragma unroll
+#pragma unroll 1  // one copy of the reconstruction code: the kernel fits the instruction cache
     for (int l = 0; l < HG_NPR; l++)
       strip_recon_f32<RS, d == 0, NF>(G, G.p32 + l * G.S + o0 - 3 * st, st, l, i0, nf, sm, 2 * NF * l,
                                       2 * NF * l + NF, tx);
