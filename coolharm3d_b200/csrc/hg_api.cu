@@ -124,6 +124,10 @@ static int validate(const hg_grid_desc *d)
   if (d->n1 < 1 || d->n2 < 1 || d->n3 < 1) return HG_ERR_BADARG;
   if (d->n1 + 2 * HG_NGH >= (1 << 21) || d->n2 + 2 * HG_NGH >= (1 << 21) || d->n3 + 2 * HG_NGH >= (1 << 21))
     return HG_ERR_BADARG;
+  // the kernels index zones and faces with 32-bit arithmetic: every plane
+  // must hold fewer than 2^31 entries (2^31 zones would need ~1 TB of HBM)
+  if ((long long)(d->n1 + 2 * HG_NGH) * (d->n2 + 2 * HG_NGH) * (d->n3 + 2 * HG_NGH) >= (1LL << 31))
+    return HG_ERR_BADARG;
   if (d->recon_type < 0 || d->recon_type > 5) return HG_ERR_BADARG;
   if (d->flux_type != 0 && d->flux_type != 1) return HG_ERR_BADARG;
   if (d->bc_type != 0 && d->bc_type != 1 && d->bc_type != 10) return HG_ERR_BADARG;

@@ -187,12 +187,13 @@ template <bool RS, int MDIM, int d>
 __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux(const __grid_constant__ GridDev G, const double *__restrict__ ph,
                                                  int lo0, int lo1, int lo2, int n0, int n1, int n2, unsigned int mult)
 {
-  const long total = (long)n0 * n1 * n2;
+  const unsigned total = (unsigned)n0 * n1 * n2;  // < 2^31 (hg_init)
   double vmax = 0.;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int i = lo0 + (int)(t % n0);
-    const int j = lo1 + (int)((t / n0) % n1);
-    const int k = lo2 + (int)(t / ((long)n0 * n1));
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned tq = t / (unsigned)n0;
+    const int i = lo0 + (int)(t - tq * (unsigned)n0);
+    const int j = lo1 + (int)(tq % (unsigned)n1);
+    const int k = lo2 + (int)(tq / (unsigned)n1);
     double pl[HG_NPR], pr[HG_NPR];
     face_prims<RS>(G, ph, d, i, j, k, pl, pr);
     double ctop;
@@ -297,22 +298,22 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux_strip(const __gri
   // lanes take consecutive strips of the same line
   const int nd = (d == 0) ? n0 : (d == 1) ? n1 : n2;
   const int nseg = (nd + NF - 1) / NF;
-  const long total = (long)nseg * (d == 0 ? (long)n1 * n2 : d == 1 ? (long)n0 * n2 : (long)n0 * n1);
+  const unsigned total = (unsigned)nseg * (d == 0 ? n1 * n2 : d == 1 ? n0 * n2 : n0 * n1);  // < 2^31 (hg_init)
   const long st = G.st[d];
   double vmax = 0.;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     int seg, i0, j0, k0;
     if (d == 0) {
-      seg = (int)(t % nseg);
-      const long rest = t / nseg;
+      const unsigned rest = t / (unsigned)nseg;
+      seg = (int)(t - rest * (unsigned)nseg);
       i0 = lo0 + seg * NF;
-      j0 = lo1 + (int)(rest % n1);
-      k0 = lo2 + (int)(rest / n1);
+      j0 = lo1 + (int)(rest % (unsigned)n1);
+      k0 = lo2 + (int)(rest / (unsigned)n1);
     } else {
-      i0 = lo0 + (int)(t % n0);
-      const long rest = t / n0;
-      seg = (int)(rest % nseg);
-      const int other = (int)(rest / nseg);
+      const unsigned rest = t / (unsigned)n0;
+      i0 = lo0 + (int)(t - rest * (unsigned)n0);
+      const unsigned other = rest / (unsigned)nseg;
+      seg = (int)(rest - other * (unsigned)nseg);
       j0 = (d == 1) ? lo1 + seg * NF : lo1 + other;
       k0 = (d == 1) ? lo2 + other : lo2 + seg * NF;
     }
@@ -371,13 +372,14 @@ __device__ __forceinline__ void line_edges(const GridDev &G, const double *__res
 
 __global__ void __launch_bounds__(HG_BLK) k_emf(GridDev G, int lo0, int lo1, int lo2, int n0, int n1, int n2)
 {
-  const long total = (long)n0 * n1 * n2;
+  const unsigned total = (unsigned)n0 * n1 * n2;  // < 2^31 (hg_init)
   const double *F0 = G.F[0], *F1 = G.F[1], *F2 = G.F[2];
   const long S = G.S;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int i = lo0 + (int)(t % n0);
-    const int j = lo1 + (int)((t / n0) % n1);
-    const int k = lo2 + (int)(t / ((long)n0 * n1));
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned tq = t / (unsigned)n0;
+    const int i = lo0 + (int)(t - tq * (unsigned)n0);
+    const int j = lo1 + (int)(tq % (unsigned)n1);
+    const int k = lo2 + (int)(tq / (unsigned)n1);
     const long o = off3(G, i, j, k);
     double e0, e1, e2;
     if (G.ct_para) {
@@ -509,16 +511,17 @@ template <bool RS, int MDIM>
 __global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __grid_constant__ GridDev G, int sub,
                                                                     double dtfac, const double *__restrict__ p_h)
 {
-  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
-  const long total = (long)N0 * N1 * N2;
+  const unsigned N0 = G.N[0], N1 = G.N[1];
+  const unsigned total = (unsigned)G.capacity;  // < 2^31 (hg_init)
   const double Dt = dtfac * G.sc->dt;
   const long S = G.S;
   const double *p = G.p;
   double msum = 0.;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int i = HG_NGH + (int)(t % N0);
-    const int j = HG_NGH + (int)((t / N0) % N1);
-    const int k = HG_NGH + (int)(t / ((long)N0 * N1));
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned tq = t / N0;
+    const int i = HG_NGH + (int)(t - tq * N0);
+    const int j = HG_NGH + (int)(tq % N1);
+    const int k = HG_NGH + (int)(tq / N1);
     const long o = off3(G, i, j, k);
     Geom gl;
     if (MDIM != 0) load_geom(G, 3, i, j, gl);
@@ -557,15 +560,16 @@ template <bool RS, int MDIM>
 __global__ void __launch_bounds__(HG_BLK, HG_C2P_MINB) k_update_c2p(const __grid_constant__ GridDev G, int sub,
                                                                    double *__restrict__ p_f)
 {
-  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
-  const long total = (long)N0 * N1 * N2;
+  const unsigned N0 = G.N[0], N1 = G.N[1];
+  const unsigned total = (unsigned)G.capacity;  // < 2^31 (hg_init)
   const long S = G.S;
   const double *p = G.p;
   unsigned int n_full = 0, n_floor = 0;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int i = HG_NGH + (int)(t % N0);
-    const int j = HG_NGH + (int)((t / N0) % N1);
-    const int k = HG_NGH + (int)(t / ((long)N0 * N1));
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned tq = t / N0;
+    const int i = HG_NGH + (int)(t - tq * N0);
+    const int j = HG_NGH + (int)(tq % N1);
+    const int k = HG_NGH + (int)(tq / N1);
     const long o = off3(G, i, j, k);
     Geom gl;
     if (MDIM != 0) load_geom(G, 3, i, j, gl);
@@ -1072,13 +1076,14 @@ __global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict_
 // (init.torus.c:205-215).
 __global__ void __launch_bounds__(HG_BLK) k_fixup_cells(GridDev G)
 {
-  const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
-  const long total = (long)N0 * N1 * N2;
+  const unsigned N0 = G.N[0], N1 = G.N[1];
+  const unsigned total = (unsigned)G.capacity;  // < 2^31 (hg_init)
   const long S = G.S;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int i = HG_NGH + (int)(t % N0);
-    const int j = HG_NGH + (int)((t / N0) % N1);
-    const int k = HG_NGH + (int)(t / ((long)N0 * N1));
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned tq = t / N0;
+    const int i = HG_NGH + (int)(t - tq * N0);
+    const int j = HG_NGH + (int)(tq % N1);
+    const int k = HG_NGH + (int)(tq / N1);
     const long o = off3(G, i, j, k);
     Geom g;
     if (G.mdim != 0) load_geom(G, 3, i, j, g);
@@ -1586,7 +1591,7 @@ __global__ void __launch_bounds__(HG_BLK) k_flux_noalloc(const __grid_constant__
                                                          int n0, int n1, int n2, double *max_out,
                                                          unsigned long long *scratch)
 {
-  const long total = (long)n0 * n1 * n2;
+  const unsigned total = (unsigned)n0 * n1 * n2;  // < 2^31 (hg_init)
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double vmax = 0.;
   if (t < total) {

@@ -127,14 +127,15 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_f32(const __gri
                                                                     int lo1, int lo2, int n0, int n1, int n2,
                                                                     unsigned int mult)
 {
-  const long total = (long)n0 * n1 * n2;
+  const unsigned total = (unsigned)n0 * n1 * n2;  // < 2^31 (hg_init)
   const int dim = d + 1;
   const float gam = (float)G.gam;
   double vmax = 0.;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int i = lo0 + (int)(t % n0);
-    const int j = lo1 + (int)((t / n0) % n1);
-    const int k = lo2 + (int)(t / ((long)n0 * n1));
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned tq = t / (unsigned)n0;
+    const int i = lo0 + (int)(t - tq * (unsigned)n0);
+    const int j = lo1 + (int)(tq % (unsigned)n1);
+    const int k = lo2 + (int)(tq / (unsigned)n1);
     const long o = off3(G, i, j, k);
     float pl[HG_NPR], pr[HG_NPR];
     face_prims_f32<RS>(G, d, i, j, k, pl, pr);
@@ -278,22 +279,22 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const
   const int tx = threadIdx.x;
   const int nd = (d == 0) ? n0 : (d == 1) ? n1 : n2;
   const int nseg = (nd + NF - 1) / NF;
-  const long total = (long)nseg * (d == 0 ? (long)n1 * n2 : d == 1 ? (long)n0 * n2 : (long)n0 * n1);
+  const unsigned total = (unsigned)nseg * (d == 0 ? n1 * n2 : d == 1 ? n0 * n2 : n0 * n1);  // < 2^31 (hg_init)
   const long st = G.st[d];
   double vmax = 0.;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     int seg, i0, j0, k0;
     if (d == 0) {  // consecutive lanes on consecutive strips of a line
-      seg = (int)(t % nseg);
-      const long rest = t / nseg;
+      const unsigned rest = t / (unsigned)nseg;
+      seg = (int)(t - rest * (unsigned)nseg);
       i0 = lo0 + seg * NF;
-      j0 = lo1 + (int)(rest % n1);
-      k0 = lo2 + (int)(rest / n1);
+      j0 = lo1 + (int)(rest % (unsigned)n1);
+      k0 = lo2 + (int)(rest / (unsigned)n1);
     } else {  // lanes along x1
-      i0 = lo0 + (int)(t % n0);
-      const long rest = t / n0;
-      seg = (int)(rest % nseg);
-      const int other = (int)(rest / nseg);
+      const unsigned rest = t / (unsigned)n0;
+      i0 = lo0 + (int)(t - rest * (unsigned)n0);
+      const unsigned other = rest / (unsigned)nseg;
+      seg = (int)(rest - other * (unsigned)nseg);
       j0 = (d == 1) ? lo1 + seg * NF : lo1 + other;
       k0 = (d == 1) ? lo2 + other : lo2 + seg * NF;
     }
