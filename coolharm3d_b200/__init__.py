@@ -226,10 +226,14 @@ class Engine:
         assert p.shape == self.shape + (NP,), p.shape
         _check(self.lib.hg_upload_prims(self.h, _ptr(p)), "hg_upload_prims")
 
-    def download(self):
-        p = np.empty(self.shape + (NP,))
-        _check(self.lib.hg_download_prims(self.h, _ptr(p)), "hg_download_prims")
-        return p
+    def download(self, out=None):
+        """The primitives in the reference layout; into `out` (a C-contiguous
+        float64 array of that shape, e.g. from pinned_array) if given."""
+        if out is None:
+            out = np.empty(self.shape + (NP,))
+        assert out.shape == self.shape + (NP,) and out.dtype == np.float64 and out.flags.c_contiguous
+        _check(self.lib.hg_download_prims(self.h, _ptr(out)), "hg_download_prims")
+        return out
 
     def set_time(self, t, dt):
         _check(self.lib.hg_set_time(self.h, t, dt), "hg_set_time")
@@ -336,6 +340,15 @@ def mem_info(device=0):
     f, t = ctypes.c_uint64(), ctypes.c_uint64()
     _check(load_library().hg_mem_info(device, ctypes.byref(f), ctypes.byref(t)), "hg_mem_info")
     return f.value, t.value
+
+
+def pinned_array(shape, dtype=np.float64):
+    """A numpy array in page-locked host memory (torch's pinned allocator).
+    hg_upload_prims / hg_download_prims move such a buffer by one DMA, with
+    no staging copy on the host."""
+    import torch
+    t = torch.empty(int(np.prod(shape)) * np.dtype(dtype).itemsize, dtype=torch.uint8, pin_memory=True)
+    return t.numpy().view(dtype).reshape(shape)  # the view's base chain holds the tensor
 
 
 def grid_bytes(desc):

@@ -471,18 +471,36 @@ static cudaError_t run_workers(long nch, W work)
   return cudaSuccess;
 }
 
-// FILL(dst, first zone, zones) writes that many zones of the reference order
+// True if the whole range [p, p + bytes) lies in page-locked host memory
+// (cudaHostAlloc or cudaHostRegister): the DMA engines can then read or
+// write the caller's buffer directly, with no staging copy on the host.
+static bool host_pinned(const void *p, size_t bytes)
+{
+  cudaPointerAttributes a, b;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess ||
+      cudaPointerGetAttributes(&b, (const char *)p + bytes - 1) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost && b.type == cudaMemoryTypeHost;
+}
+
+// FILL(dst, first zone, zones) writes that many zones of the reference order;
+// with a page-locked `direct` source the reference-order array is copied by
+// one DMA instead.
 template <class FILL>
-static int upload_impl(hg_handle *h, FILL fill)
+static int upload_impl(hg_handle *h, FILL fill, const double *direct = nullptr)
 {
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
   double *dref = ref_buffer(h);
   if (!dref) return HG_ERR_NOMEM;
   const long zc = HG_XCH_BYTES / (sizeof(double) * HG_NPR);  // zones per chunk
-  const long nch = (h->ntot_ref + zc - 1) / zc;
+  const long nch = direct ? 0 : (h->ntot_ref + zc - 1) / zc;
   const int dev = h->d.device;
-  HG_CK(run_workers(nch, [&](int w, int nw) -> cudaError_t {
+  if (direct)
+    HG_CK(cudaMemcpyAsync(dref, direct, sizeof(double) * HG_NPR * h->ntot_ref, cudaMemcpyHostToDevice, h->stream));
+  else HG_CK(run_workers(nch, [&](int w, int nw) -> cudaError_t {
     cudaError_t e = cudaSetDevice(dev);
     long n = 0;
     for (long c = w; c < nch && e == cudaSuccess; c += nw, n++) {
@@ -507,9 +525,10 @@ static int upload_impl(hg_handle *h, FILL fill)
   return HG_OK;
 }
 
-// DRAIN(src, first zone, zones) reads that many zones of the reference order
+// DRAIN(src, first zone, zones) reads that many zones of the reference order;
+// a page-locked `direct` destination receives the array by one DMA instead.
 template <class DRAIN>
-static int download_impl(hg_handle *h, DRAIN drain)
+static int download_impl(hg_handle *h, DRAIN drain, double *direct = nullptr)
 {
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
@@ -517,6 +536,11 @@ static int download_impl(hg_handle *h, DRAIN drain)
   if (!dref) return HG_ERR_NOMEM;
   hg::launch_planes_to_ref(G, h->L, h->stream, G.p, h->NT[0], h->NT[1], h->NT[2], dref);
   HG_CK(cudaGetLastError());
+  if (direct) {
+    HG_CK(cudaMemcpyAsync(direct, dref, sizeof(double) * HG_NPR * h->ntot_ref, cudaMemcpyDeviceToHost, h->stream));
+    HG_CK(cudaStreamSynchronize(h->stream));
+    return HG_OK;
+  }
   const long zc = HG_XCH_BYTES / (sizeof(double) * HG_NPR);
   const long nch = (h->ntot_ref + zc - 1) / zc;
   const int dev = h->d.device;
@@ -552,17 +576,21 @@ static int download_impl(hg_handle *h, DRAIN drain)
 extern "C" int hg_upload_prims(hg_handle *h, const double *p)
 {
   if (!h || !p) return HG_ERR_BADARG;
-  return upload_impl(h, [&](double *dst, long z0, long nz) {
-    memcpy(dst, p + z0 * HG_NPR, sizeof(double) * HG_NPR * nz);
-  });
+  HG_CK(cudaSetDevice(h->d.device));
+  const bool pinned = host_pinned(p, sizeof(double) * HG_NPR * h->ntot_ref);
+  return upload_impl(
+      h, [&](double *dst, long z0, long nz) { memcpy(dst, p + z0 * HG_NPR, sizeof(double) * HG_NPR * nz); },
+      pinned ? p : nullptr);
 }
 
 extern "C" int hg_download_prims(hg_handle *h, double *p)
 {
   if (!h || !p) return HG_ERR_BADARG;
-  return download_impl(h, [&](const double *src, long z0, long nz) {
-    memcpy(p + z0 * HG_NPR, src, sizeof(double) * HG_NPR * nz);
-  });
+  HG_CK(cudaSetDevice(h->d.device));
+  const bool pinned = host_pinned(p, sizeof(double) * HG_NPR * h->ntot_ref);
+  return download_impl(
+      h, [&](const double *src, long z0, long nz) { memcpy(p + z0 * HG_NPR, src, sizeof(double) * HG_NPR * nz); },
+      pinned ? p : nullptr);
 }
 
 // zone z of the reference order -> (i, j, k)

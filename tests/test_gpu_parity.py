@@ -188,6 +188,26 @@ def test_steps_in_one_call_equal_steps_one_by_one():
     assert np.array_equal(e1.download(), s["p"])
 
 
+@pytest.mark.parametrize("name", ["torus_24x16x8_s3", "linwave_2d_16x16x1_s3"])
+def test_pinned_and_pageable_transfers_agree(name):
+    """hg_upload_prims / hg_download_prims: a page-locked host buffer goes by
+    one DMA, a pageable one through the staged chunks; the resident state and
+    the state read back are the same either way."""
+    f = fixtures.load(name)
+    e, _ = engine_for(f["n"], f["sw"], f, f["p0"], f["t0"], f["dt0"])
+    e.step(f["steps"])
+    pageable = e.download()
+    pinned = e.download(out=hg.pinned_array(pageable.shape))
+    assert np.array_equal(pinned, pageable)
+    src = hg.pinned_array(pageable.shape)
+    src[...] = f["p0"]
+    e.upload(src)
+    e.set_time(f["t0"], f["dt0"])
+    e.step(f["steps"])
+    assert np.array_equal(e.download(), pageable)
+    e.close()
+
+
 @pytest.mark.parametrize("name", ["linwave_12x10x8_s2", "linwave_noee_stress_10x8x6_s2", "balsara1_lf_n64_s20",
                                   "linwave_2d_16x16x1_s3"])
 def test_face_flux_matches_oracle(name):
