@@ -235,6 +235,27 @@ def setup(wl, device, precision=0, p_init=None):
     return e, p0
 
 
+def max_over_ranks(values, world):
+    """Element-wise maximum of `values` over all ranks (the slowest rank sets
+    every time): one all_reduce on the process group's device (the GPU under
+    NCCL, the host under gloo)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    tt = torch.tensor([float(v) for v in values], dtype=torch.float64, device=dev)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return [float(v) for v in tt.tolist()]
+
+
+def whole_job_rates(world, zones, steps, ms_max, e2e_s_max):
+    """Zone-updates/s of the whole job: every rank advances its own replica
+    of `zones` zones by `steps` steps, timed by the slowest rank (device
+    milliseconds, end-to-end seconds)."""
+    return world * zones * steps / (ms_max * 1e-3), world * zones * steps / e2e_s_max
+
+
 def run_ours(args, wl, rank, world, device):
     import coolharm3d_b200 as hg
     n = wl["n"]
@@ -289,17 +310,8 @@ def run_ours(args, wl, rank, world, device):
     e.download(out=back)
     e2e_s = time.perf_counter() - t0
     del back, host_p
-    ms_all = [ms]
-    e2e_all = [e2e_s]
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        tt = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_all, e2e_all = [float(tt[0])], [float(tt[1])]
-    ms_max, e2e_max = ms_all[0], e2e_all[0]
-    value = world * zones * args.steps / (ms_max * 1e-3)
-    e2e_val = world * zones * args.steps / e2e_max
+    ms_max, e2e_max = max_over_ranks([ms, e2e_s], world)
+    value, e2e_val = whole_job_rates(world, zones, args.steps, ms_max, e2e_max)
     state_bytes = 8 * 8 * np.prod(hg.ref_shape(n))
     out = dict(metric="zone-updates/s", value=value, unit="zone-updates/s", n_gpus=world, steps=args.steps,
                warmup=args.warmup, ms_per_step=ms_max / args.steps, higher_is_better=True, scaling="weak",
