@@ -244,7 +244,7 @@ __device__ __forceinline__ void strip_recon(const GridDev &G, const double *__re
   double y[NF + 5];
 #pragma unroll
   for (int c = 0; c < NF + 5; c++) {
-    const int cc = c < nf + 4 ? c : nf + 4;
+    const int cc = c <= 4 ? c : min(c, nf + 4);  // nf >= 1: zones 0..4 always exist
     double v = __ldg(col + cc * st);
     if (RS && !X1) v = rs_roundtrip(G, v, l, i);
     if (RS && X1) v *= G.rsc[rs_type(l) * G.T[0] + i - 3 + cc];

@@ -194,7 +194,7 @@ __device__ __forceinline__ void strip_recon_f32(const GridDev &G, const float *_
   float y[NF + 5];
 #pragma unroll
   for (int c = 0; c < NF + 5; c++) {
-    const int cc = c < nf + 4 ? c : nf + 4;
+    const int cc = c <= 4 ? c : min(c, nf + 4);  // nf >= 1: zones 0..4 always exist
     float v = __ldg(col + cc * st);
     if (RS && X1) v *= __ldg(G.rsc32 + rs_type(l) * G.T[0] + i - 3 + cc);
     y[c] = v;
