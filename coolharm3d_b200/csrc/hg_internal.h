@@ -63,7 +63,7 @@ struct GridDev {
   int N[3];          // physical zones
   int T[3];          // stored extent per direction (N+6, or 1 when degenerate)
   int deg[3];        // 1 if N == 1
-  long st[3];        // stride per direction (0 when degenerate)
+  int st[3];         // stride per direction (0 when degenerate); planes hold < 2^31 entries
   long S;            // plane size
   int NE[3];         // last physical index N+2
   int recon, flux, ct_para, bc, mdim, use_ee, cooling, rescale, nsd;

@@ -116,7 +116,7 @@ __device__ __forceinline__ void face_prims(const GridDev &G, const double *__res
     }
     return;
   }
-  const long st = G.st[d];
+  const int st = G.st[d];
 #pragma unroll
   for (int l = 0; l < HG_NPR; l++) {
     double y[6];
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux(const __grid_cons
 // it (face_prims<RS>, d = 0); along x2, x3 every value takes the
 // scale/unscale round trip of its zone i.
 template <bool RS, bool X1, int NF>
-__device__ __forceinline__ void strip_recon(const GridDev &G, const double *__restrict__ col, long st, int l, int i,
+__device__ __forceinline__ void strip_recon(const GridDev &G, const double *__restrict__ col, int st, int l, int i,
                                             int nf, double *sm, int bl, int br, int tx)
 {
   const int rt = G.recon;
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux_strip(const __gri
   const int nd = (d == 0) ? n0 : (d == 1) ? n1 : n2;
   const int nseg = (nd + NF - 1) / NF;
   const unsigned total = (unsigned)nseg * (d == 0 ? n1 * n2 : d == 1 ? n0 * n2 : n0 * n1);  // < 2^31 (hg_init)
-  const long st = G.st[d];
+  const int st = G.st[d];
   double vmax = 0.;
   for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     int seg, i0, j0, k0;
@@ -363,7 +363,7 @@ __device__ __forceinline__ void line_edges(const GridDev &G, const double *__res
     *rprev = *lcur = __ldg(f + o);
     return;
   }
-  const long st = G.st[a];
+  const int st = G.st[a];
   double y[6];
 #pragma unroll
   for (int m = 0; m < 6; m++) y[m] = __ldg(f + o + (m - 3) * st);

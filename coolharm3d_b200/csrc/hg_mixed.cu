@@ -88,7 +88,7 @@ __device__ __forceinline__ void face_prims_f32(const GridDev &G, int d, int i, i
     for (int l = 0; l < HG_NPR; l++) pl[l] = pr[l] = __ldg(ph + l * G.S + o);
     return;
   }
-  const long st = G.st[d];
+  const int st = G.st[d];
 #pragma unroll
   for (int l = 0; l < HG_NPR; l++) {
     float y[6];
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_f32(const __gri
 // X1 with RESCALE_R: zones scaled by their factors before, face states by
 // their faces' factors after the reconstruction (FP32 copies of the tables).
 template <bool RS, bool X1, int NF>
-__device__ __forceinline__ void strip_recon_f32(const GridDev &G, const float *__restrict__ col, long st, int l, int i,
+__device__ __forceinline__ void strip_recon_f32(const GridDev &G, const float *__restrict__ col, int st, int l, int i,
                                                 int nf, float *sm, int bl, int br, int tx)
 {
   const int rt = G.recon;
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const
   const int nd = (d == 0) ? n0 : (d == 1) ? n1 : n2;
   const int nseg = (nd + NF - 1) / NF;
   const unsigned total = (unsigned)nseg * (d == 0 ? n1 * n2 : d == 1 ? n0 * n2 : n0 * n1);  // < 2^31 (hg_init)
-  const long st = G.st[d];
+  const int st = G.st[d];
   double vmax = 0.;
   for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     int seg, i0, j0, k0;

@@ -31,7 +31,7 @@ struct StateT {
 };
 typedef StateT<double> State;
 
-__device__ __forceinline__ long off3(const GridDev &G, int i, int j, int k)
+__device__ __forceinline__ int off3(const GridDev &G, int i, int j, int k)  // 32-bit: planes < 2^31 entries
 {
   return i * G.st[0] + j * G.st[1] + k * G.st[2];
 }
