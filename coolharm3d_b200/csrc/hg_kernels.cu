@@ -41,6 +41,9 @@ namespace hg {
 #ifndef HG_FLUX_MINB
 #define HG_FLUX_MINB 4
 #endif
+#ifndef HG_EE_MINB
+#define HG_EE_MINB 4
+#endif
 
 // (x * rscale) * (1/rscale): the value rescale_prims_r() leaves in p_h after
 // it scaled and unscaled it around the x1 reconstruction (recon.c:1168-1200).
@@ -633,7 +636,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_C2P_MINB) k_update_c2p(const __grid
 // states of the six faces (recomputed here; the flux kernel does not store
 // them) and the inversions Utoprim_1d_ee / Utoprim_1d_ee2.
 template <bool RS>
-__device__ __noinline__ double ee_face_flux(const GridDev &G, const double *p_h, int d, int i, int j, int k)
+__device__ __forceinline__ double ee_face_flux(const GridDev &G, const double *p_h, int d, int i, int j, int k)
 {
   double pl[HG_NPR], pr[HG_NPR];
   face_prims<RS>(G, p_h, d, i, j, k, pl, pr);
@@ -666,7 +669,7 @@ __device__ __noinline__ double ee_face_flux(const GridDev &G, const double *p_h,
 // thread, ahead of k_fallback: q_F[6 e + f], f = 0..2 the lower faces of
 // x1..x3, 3..5 the upper ones.
 template <bool RS>
-__global__ void __launch_bounds__(HG_BLK) k_ee_faces(GridDev G, const double *__restrict__ p_h)
+__global__ void __launch_bounds__(HG_BLK, HG_EE_MINB) k_ee_faces(GridDev G, const double *__restrict__ p_h)
 {
   const long n = 6L * min(G.sc->q_count, (int)G.capacity);
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
