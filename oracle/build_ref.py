@@ -9,7 +9,7 @@ What it does, per configuration:
   1. stages the reference's src/ files into oracle/_ref/<cfg>/src/
      (a git-ignored build folder; reference sources are never committed),
   2. applies the documented compile-time switch edits to the staged
-     options.h (each edit is listed in CONFIGS below and in DESIGN.md),
+     options.h (each edit is listed in CONFIGS below),
      and the documented parameter edits to the staged init.<setup>.c,
   3. regenerates defs.h from globals.h exactly as the reference makefile
      does (src/makefile, the `egrep "^extern|^#if..." globals.h | sed` rule),

@@ -2,8 +2,9 @@
  *
  * This is the oracle: a plain-C restatement of the reference's step_ch()/
  * advance() path (src/step_ch.c:50-451 of scnastro/coolharm3d), used only by
- * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg as the
- * checker.  The product (coolharm3d_b200/) never links or calls it.
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg, to verify
+ * the engine's results.  The product (coolharm3d_b200/) never links or calls
+ * it.
  *
  * Parity pin: tests/test_oracle_vs_reference.py runs the reference's own CPU
  * build (oracle/_ref, made by oracle/build_ref.py) and this restatement on
