@@ -41,7 +41,7 @@ class GridDesc(ctypes.Structure):
                 ("t", ctypes.c_double), ("device", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
-EXPORTS = ["hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", "hg_download_prims",
+EXPORTS = ["hg_check_mirror", "hg_init", "hg_set_geometry", "hg_set_cell_data", "hg_upload_prims", "hg_download_prims",
            "hg_upload_prims_tree", "hg_download_prims_tree", "hg_set_time", "hg_step", "hg_get_fail_counts",
            "hg_download_pflag", "hg_download_gamma", "hg_download_nfail", "hg_get_diag", "hg_last_step_ms",
            "hg_destroy", "hg_strerror", "hg_build_geometry_minkowski", "hg_profile", "hg_kernel_times", "hg_face_flux", "hg_face_flux_noalloc", "hg_set_cooling_tables",
@@ -82,6 +82,7 @@ def load_library(path=LIB_PATH):
                "hg_get_fail_counts", "hg_download_pflag", "hg_download_gamma", "hg_download_nfail",
                "hg_last_step_ms"):
         getattr(lib, fn).argtypes = [P, P]
+    lib.hg_check_mirror.argtypes = [P, P, P]
     lib.hg_set_time.argtypes = [P, ctypes.c_double, ctypes.c_double]
     lib.hg_step.argtypes = [P, ctypes.c_int32, P, P]
     lib.hg_get_diag.argtypes = [P, P, P]
@@ -225,6 +226,14 @@ class Engine:
         p = np.ascontiguousarray(p, np.float64)
         assert p.shape == self.shape + (NP,), p.shape
         _check(self.lib.hg_upload_prims(self.h, _ptr(p)), "hg_upload_prims")
+
+    def check_mirror(self, first=False):
+        """Mixed form: stored values where the FP32 copy differs from the
+        state rounded to float (0 expected between steps); with first=True
+        also the lowest mismatching stored offset (l * S + o), or -1."""
+        n, f = ctypes.c_int64(), ctypes.c_int64()
+        _check(self.lib.hg_check_mirror(self.h, ctypes.byref(n), ctypes.byref(f)), "hg_check_mirror")
+        return (n.value, f.value) if first else n.value
 
     def download(self, out=None):
         """The primitives in the reference layout; into `out` (a C-contiguous

@@ -22,6 +22,8 @@
 namespace hg {
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R);
 void *gather_times_kernel();
+void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
+void launch_mirror_check(const GridDev &G, int grid, cudaStream_t s, const double *src, unsigned long long *count);
 void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d);
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
@@ -1058,6 +1060,24 @@ extern "C" void hg_batch_destroy(hg_batch *b)
 }
 
 // ---------------------------------------------------------------------------
+extern "C" int hg_check_mirror(hg_handle *h, int64_t *mismatches, int64_t *first)
+{
+  if (!h || !mismatches) return HG_ERR_BADARG;
+  if (!h->G.p32) return HG_ERR_BADARG;  // the FP64 form keeps no FP32 copy
+  HG_CK(cudaSetDevice(h->d.device));
+  unsigned long long *d = nullptr, n[2] = {0ull, ~0ull};
+  HG_CK(cudaMallocAsync((void **)&d, sizeof(n), h->stream));
+  HG_CK(cudaMemcpyAsync(d, n, sizeof(n), cudaMemcpyHostToDevice, h->stream));
+  hg::launch_mirror_check(h->G, h->L.grid_upd, h->stream, h->G.p, d);
+  HG_CK(cudaGetLastError());
+  HG_CK(cudaMemcpyAsync(n, d, sizeof(n), cudaMemcpyDeviceToHost, h->stream));
+  HG_CK(cudaFreeAsync(d, h->stream));
+  HG_CK(cudaStreamSynchronize(h->stream));
+  *mismatches = (int64_t)n[0];
+  if (first) *first = n[0] ? (int64_t)n[1] : -1;
+  return HG_OK;
+}
+
 extern "C" int hg_mem_info(int32_t device, uint64_t *free_bytes, uint64_t *total_bytes)
 {
   size_t f = 0, t = 0;
@@ -1193,6 +1213,8 @@ static int snap(hg_handle *h, Snapshot &s, bool save)
   HG_CK(cp(s.pflag, G.pflag, sizeof(int) * G.S));
   HG_CK(cp(s.nfail, G.nfail, sizeof(unsigned int) * G.S * HG_NF));
   HG_CK(cp(s.sc, G.sc, sizeof(hg::DevScalars)));
+  if (!save && G.p32) hg::launch_to_f32(G, h->L.grid_upd, h->stream, G.p);  // the FP32 copy of the restored state
+  HG_CK(cudaGetLastError());
   HG_CK(cudaStreamSynchronize(h->stream));
   return HG_OK;
 }

@@ -9,6 +9,17 @@ namespace hg {
 
 __device__ __forceinline__ int rs_type(int l) { return l == RHO ? 0 : (l == UU ? 2 : 1); }
 
+// One value of the state written at plane offset `at` (l * S + o).  The
+// mixed form keeps the FP32 copy its flux kernels read in step with every
+// write, so no conversion pass runs before each substep: whichever array a
+// step kernel writes (ph in the predictor, p in the corrector) is the next
+// substep's flux input.
+__device__ __forceinline__ void put_state(const GridDev &G, double *a, long at, double v)
+{
+  a[at] = v;
+  if (G.p32) G.p32[at] = (float)v;
+}
+
 __device__ __forceinline__ void block_max_atomic(double v, unsigned long long *dst)
 {
   __shared__ double red[HG_BLK / 32];

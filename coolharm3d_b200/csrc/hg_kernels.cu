@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_C2P_MINB) k_update_c2p(const __grid
     G.p_gamma[o] = gamma;
     if (pflag == PF_NONE) G.pflag[o] = PF_NONE;
 #pragma unroll
-    for (int l = 0; l < HG_NPR; l++) p_f[l * S + o] = pf[l];
+    for (int l = 0; l < HG_NPR; l++) put_state(G, p_f, l * S + o, pf[l]);
   }
   const unsigned int c_full = block_count(n_full);
   const unsigned int c_floor = block_count(n_floor);
@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(HG_BLK) k_fallback(GridDev G, int sub, double 
     G.p_gamma[o] = pgam;
     if (pflag != PF_NONE) flag_zone(G, pflag, i, j, k);
     else G.pflag[o] = PF_NONE;
-    for (int l = 0; l < HG_NPR; l++) p_f[l * S + o] = pf[l];
+    for (int l = 0; l < HG_NPR; l++) put_state(G, p_f, l * S + o, pf[l]);
   }
 }
 
@@ -882,7 +882,7 @@ __device__ __forceinline__ void bounds_spherical3(const GridDev &G, double *__re
     v[B2] *= -1;
   }
 #pragma unroll
-  for (int l = 0; l < HG_NPR; l++) pa[l * G.S + od] = v[l];
+  for (int l = 0; l < HG_NPR; l++) put_state(G, pa, l * G.S + od, v[l]);
 }
 
 __global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict__ pa, int conditional)
@@ -931,7 +931,7 @@ __global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict
     const int sk = G.deg[2] ? k : bc_map(k, N2, per);
     const long os = (long)si * G.st[0] + (long)sj * G.st[1] + (long)sk * G.st[2];
 #pragma unroll
-    for (int l = 0; l < HG_NPR; l++) pa[l * S + od] = pa[l * S + os];
+    for (int l = 0; l < HG_NPR; l++) put_state(G, pa, l * S + od, pa[l * S + os]);
     // pflag ghosts are copies while a failure exists in this substep; otherwise
     // every pflag of the reference is zero (step_ch.c:65-69, 123-127)
     G.pflag[od] = fl ? G.pflag[os] : 0;
@@ -990,7 +990,7 @@ __global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict_
       G.p_gamma[o] = HG_GAMMAMAX;
       book(G, NF_GAMMA_MAX, ci, cj, ck);
       book(G, NF_INTERP_V, ci, cj, ck);
-      for (int l = U1; l <= U3; l++) pv[l * S + o] = pc[l];
+      for (int l = U1; l <= U3; l++) put_state(G, pv, l * S + o, pc[l]);
       continue;
     }
     for (int l = lo; l <= hi; l++) pc[l] = 0.;
@@ -1066,7 +1066,7 @@ __global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict_
         G.p_gamma[o] = gamma;
       }
     }
-    for (int l = lo; l <= hi; l++) pv[l * S + o] = pc[l];
+    for (int l = lo; l <= hi; l++) put_state(G, pv, l * S + o, pc[l]);
   }
 }
 
@@ -1275,7 +1275,7 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
   const double dtfac = sub == 0 ? 0.5 : 1.0;
   mark(R, KC_MISC, s);
   k_begin<<<1, 1, 0, s>>>(G.sc);
-  if (G.prec == HG_PREC_MIXED) launch_to_f32(G, L.grid_upd, s, ph);
+  // (the mixed form's FP32 copy of ph is already current: put_state)
   for (int d = 0; d < 3; d++) launch_flux_dir(G, L, s, ph, d, R);
   {
     int lo[3], n[3];
@@ -1358,6 +1358,7 @@ void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, 
                           double *out)
 {
   k_ref_to_planes<<<L.grid_flux, HG_BLK, 0, s>>>(G, ref, NT1, NT2, out);
+  if (G.p32 && out == G.p) launch_to_f32(G, L.grid_upd, s, G.p);  // the state set from the host
 }
 
 void launch_planes_to_ref(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *in, int NT0, int NT1,
@@ -1379,6 +1380,7 @@ void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
   k_begin<<<1, 1, 0, s>>>(G.sc);
   k_fixup_cells<<<L.grid_upd, HG_BLK, 0, s>>>(G);
   k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0);
+  if (G.p32) launch_to_f32(G, L.grid_upd, s, G.p);  // the FP32 copy of the state set from the host
 }
 
 // ---------------------------------------------------------------------------
@@ -1530,6 +1532,7 @@ void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
 {
   k_begin<<<1, 1, 0, s>>>(G.sc);
   k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0);
+  if (G.p32) launch_to_f32(G, L.grid_upd, s, G.p);
 }
 
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R)

@@ -122,6 +122,34 @@ void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src
   k_to_f32<<<grid, HG_BLK, 0, s>>>(G, src);
 }
 
+// Stored values where the FP32 copy differs from the state rounded to float
+// (hg_check_mirror): zero after every step and every host update.
+// count[0]: mismatches, count[1]: the lowest mismatching offset (l * S + o).
+// Compared as FP32 values in this flush-to-zero unit, as the FP32 flux
+// kernels read them: a subnormal written by an FP64 kernel's conversion
+// equals the zero this unit's conversion gives.
+__global__ void __launch_bounds__(HG_BLK) k_mirror_check(GridDev G, const double *__restrict__ src,
+                                                        unsigned long long *count)
+{
+  const long total = (long)HG_NPR * G.S;
+  const long stride = (long)gridDim.x * blockDim.x;
+  unsigned long long n = 0, first = ~0ull;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += stride)
+    if (G.p32[t] != (float)src[t]) {
+      n++;
+      if ((unsigned long long)t < first) first = (unsigned long long)t;
+    }
+  if (n) {
+    atomicAdd(count, n);
+    atomicMin(count + 1, first);
+  }
+}
+
+void launch_mirror_check(const GridDev &G, int grid, cudaStream_t s, const double *src, unsigned long long *count)
+{
+  k_mirror_check<<<grid, HG_BLK, 0, s>>>(G, src, count);
+}
+
 template <bool RS, int MDIM, int d>
 __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_f32(const __grid_constant__ GridDev G, int lo0,
                                                                     int lo1, int lo2, int n0, int n1, int n2,

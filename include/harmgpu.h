@@ -234,6 +234,14 @@ int hg_kernel_times(hg_handle *h, double ms[HG_NKCLASS], int64_t launches[HG_NKC
  * hg_init will allocate for a description: what a server admitting grids by
  * free memory needs.  No reference counterpart. */
 int hg_mem_info(int32_t device, uint64_t *free_bytes, uint64_t *total_bytes);
+/* Mixed form only (HG_ERR_BADARG otherwise): the number of stored values
+ * where the FP32 copy of the state the FP32 flux kernels read differs from
+ * the FP64 state rounded to float.  Every step kernel that writes the state
+ * writes the copy too, and every host update refreshes it, so this is 0
+ * between steps; *first (may be NULL) receives the lowest mismatching
+ * offset l * S + o in the stored planes, or -1.  No reference counterpart (a
+ * consistency check). */
+int hg_check_mirror(hg_handle *h, int64_t *mismatches, int64_t *first);
 int hg_grid_bytes(const hg_grid_desc *desc, uint64_t *bytes);
 
 typedef struct hg_batch hg_batch;

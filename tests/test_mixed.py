@@ -124,3 +124,29 @@ def test_mixed_launch_configurations_agree():
     for p in runs[1:]:
         err = l1_rel(p, runs[0])
         assert max(err.values()) < 1e-5, err
+
+
+@pytest.mark.parametrize("name", ["torus_stress_16x24x6_s1", "linwave_stress_10x8x6_s2", "balsara1_stress_n64_s1"])
+def test_fp32_copy_stays_current(name):
+    """The FP32 copy the mixed form's flux kernels read is written by every
+    kernel that writes the state and refreshed by every host update, so it
+    equals the FP64 state rounded to float after the set-up, after steps
+    (fixups and boundaries included), after autotuning and in a batch."""
+    f = fixtures.load(name)
+    e = fixture_engine(f, hg.PREC_MIXED)
+    assert e.check_mirror() == 0
+    for _ in range(3):
+        e.step(1)
+        assert e.check_mirror() == 0
+    e.autotune(steps=1)
+    assert e.check_mirror() == 0
+    e.fixup_bounds()
+    assert e.check_mirror() == 0
+    b = hg.Batch(0, 4)
+    b.add(e)
+    b.step()
+    assert e.check_mirror() == 0
+    b.remove(e)
+    b.close()
+    assert e.fail_counts().sum() > 0  # the stress state drives the fallback and fixup kernels
+    e.close()
