@@ -21,7 +21,9 @@
 
 namespace hg {
 
-#define HG_FLUX32_MINB 6
+#ifndef HG_FLUX32_MINB
+#define HG_FLUX32_MINB 6  // blocks of 128 per SM for the FP32 flux kernels (80 registers)
+#endif
 
 // The face's geometry in float: the entries get_state and vchar_fast read
 // (gcov, three gcon entries, ncon^0, beta, sqrt(-g)).
