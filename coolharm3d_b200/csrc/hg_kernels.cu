@@ -890,32 +890,35 @@ __global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict
   if (conditional && !G.sc->bnd_phys) return;
   const int T0 = G.T[0], T1 = G.T[1], T2 = G.T[2];
   const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
-  const long c1 = (long)T0 * T1 * (T2 - (G.deg[2] ? 1 : N2));
-  const long c2 = (long)T0 * (T1 - (G.deg[1] ? 1 : N1)) * (G.deg[2] ? 1 : N2);
-  const long c3 = (long)(T0 - (G.deg[0] ? 1 : N0)) * (G.deg[1] ? 1 : N1) * (G.deg[2] ? 1 : N2);
-  const long total = c1 + c2 + c3;
+  // ghost zones: x3 slabs, then x2 slabs, then x1 slabs (32-bit counts:
+  // fewer than the 2^31 stored zones hg_init allows)
+  const unsigned c1 = (unsigned)T0 * T1 * (T2 - (G.deg[2] ? 1 : N2));
+  const unsigned c2 = (unsigned)T0 * (T1 - (G.deg[1] ? 1 : N1)) * (G.deg[2] ? 1 : N2);
+  const unsigned c3 = (unsigned)(T0 - (G.deg[0] ? 1 : N0)) * (G.deg[1] ? 1 : N1) * (G.deg[2] ? 1 : N2);
+  const unsigned total = c1 + c2 + c3;
   const int per = (G.bc == 1);
   const int fl = G.sc->failure_exists;
   const long S = G.S;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     int i, j, k;  // stored indices
     if (t < c1) {
-      i = (int)(t % T0);
-      j = (int)((t / T0) % T1);
-      const int kg = (int)(t / ((long)T0 * T1));
+      const unsigned q = t / (unsigned)T0;
+      i = (int)(t - q * (unsigned)T0);
+      j = (int)(q % (unsigned)T1);
+      const int kg = (int)(q / (unsigned)T1);
       k = kg < HG_NGH ? kg : kg + N2;
     } else if (t < c1 + c2) {
-      const long u = t - c1;
-      i = (int)(u % T0);
-      const int jg = (int)((u / T0) % (T1 - N1));
+      const unsigned u = t - c1, q = u / (unsigned)T0, w = (unsigned)(T1 - N1);
+      i = (int)(u - q * (unsigned)T0);
+      const int jg = (int)(q % w);
       j = jg < HG_NGH ? jg : jg + N1;
-      k = HG_NGH + (int)(u / ((long)T0 * (T1 - N1)));
+      k = HG_NGH + (int)(q / w);
     } else {
-      const long u = t - c1 - c2;
-      const int ig = (int)(u % (T0 - N0));
+      const unsigned u = t - c1 - c2, w = (unsigned)(T0 - N0), q = u / w;
+      const int ig = (int)(u - q * w);
       i = ig < HG_NGH ? ig : ig + N0;
-      j = HG_NGH + (int)((u / (T0 - N0)) % N1);
-      k = HG_NGH + (int)(u / ((long)(T0 - N0) * N1));
+      j = HG_NGH + (int)(q % (unsigned)N1);
+      k = HG_NGH + (int)(q / (unsigned)N1);
     }
     // degenerate directions have no ghosts, so these are reference indices
     const long od = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
