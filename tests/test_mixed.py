@@ -150,3 +150,21 @@ def test_fp32_copy_stays_current(name):
     b.close()
     assert e.fail_counts().sum() > 0  # the stress state drives the fallback and fixup kernels
     e.close()
+
+
+@pytest.mark.parametrize("kind,n", [("balsara", 1024), ("field_loop", 128)])
+def test_mixed_keeps_transverse_components_zero(kind, n):
+    """A shock tube along x1 and a field loop in the x1-x2 plane have U3 =
+    B3 = 0 exactly in the FP64 form; every FP32 product that feeds them has
+    an exact zero factor, so the mixed form must keep them exactly zero."""
+    from coolharm3d_b200 import setups
+    prob = setups.balsara1(n, precision=hg.PREC_MIXED) if kind == "balsara" else \
+        setups.field_loop((n, n, 1), precision=hg.PREC_MIXED)
+    e = hg.Engine(prob.desc)
+    setups.start(e, prob)
+    e.step(100)
+    p = e.download()
+    assert np.abs(p[..., 2:4]).max() > 0 or np.abs(p[..., 5:7]).max() > 0  # the flow evolved
+    assert not p[..., 4].any() and not p[..., 7].any()
+    assert e.check_mirror() == 0
+    e.close()
