@@ -1357,17 +1357,93 @@ __global__ void __launch_bounds__(HG_BLK) k_planes_to_ref(GridDev G, const doubl
   }
 }
 
+// The same conversions when x1 and x3 both have ghosts (the usual 3D grid):
+// the reference runs k fastest and the planes i fastest, so each block
+// transposes a 32 (k) x 32 (i) tile of one x2 row through shared memory,
+// four variables at a time; both sides are then read and written in
+// contiguous runs.  grid (tiles of k, tiles of i, rows j), block (32, 8).
+#define HG_TT 32
+__global__ void __launch_bounds__(HG_TT * 8) k_ref_to_planes_tiled(GridDev G, const double *__restrict__ ref, int NT1,
+                                                                 int NT2, double *__restrict__ out)
+{
+  __shared__ double tile[4][HG_TT][HG_TT + 1];
+  const int k0 = blockIdx.x * HG_TT, i0 = blockIdx.y * HG_TT, j = blockIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int T0 = G.T[0], T2 = G.T[2];
+  const int rj = G.deg[1] ? HG_NGH : j;
+  for (int lg = 0; lg < HG_NPR; lg += 4) {
+    for (int ii = ty; ii < HG_TT; ii += 8) {
+      const int i = i0 + ii, k = k0 + tx;
+      if (i < T0 && k < T2) {
+        const double *src = ref + (((long)i * NT1 + rj) * NT2 + k) * HG_NPR + lg;
+#pragma unroll
+        for (int v = 0; v < 4; v++) tile[v][tx][ii] = src[v];
+      }
+    }
+    __syncthreads();
+    for (int kk = ty; kk < HG_TT; kk += 8) {
+      const int i = i0 + tx, k = k0 + kk;
+      if (i < T0 && k < T2) {
+        const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+#pragma unroll
+        for (int v = 0; v < 4; v++) out[(lg + v) * G.S + o] = tile[v][kk][tx];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// grid (tiles of k, tiles of i, reference rows rj over NT1), block (32, 8);
+// a degenerate x2 reads its one stored row for every reference copy
+__global__ void __launch_bounds__(HG_TT * 8) k_planes_to_ref_tiled(GridDev G, const double *__restrict__ in, int NT1,
+                                                                 int NT2, double *__restrict__ ref)
+{
+  __shared__ double tile[4][HG_TT][HG_TT + 1];
+  const int k0 = blockIdx.x * HG_TT, i0 = blockIdx.y * HG_TT, rj = blockIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int T0 = G.T[0], T2 = G.T[2];
+  const int j = G.deg[1] ? 0 : rj;
+  for (int lg = 0; lg < HG_NPR; lg += 4) {
+    for (int kk = ty; kk < HG_TT; kk += 8) {
+      const int i = i0 + tx, k = k0 + kk;
+      if (i < T0 && k < T2) {
+        const long o = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
+#pragma unroll
+        for (int v = 0; v < 4; v++) tile[v][kk][tx] = in[(lg + v) * G.S + o];
+      }
+    }
+    __syncthreads();
+    for (int ii = ty; ii < HG_TT; ii += 8) {
+      const int i = i0 + ii, k = k0 + tx;
+      if (i < T0 && k < T2) {
+        double *dst = ref + (((long)i * NT1 + rj) * NT2 + k) * HG_NPR + lg;
+#pragma unroll
+        for (int v = 0; v < 4; v++) dst[v] = tile[v][tx][ii];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
                           double *out)
 {
-  k_ref_to_planes<<<L.grid_flux, HG_BLK, 0, s>>>(G, ref, NT1, NT2, out);
+  if (!G.deg[0] && !G.deg[2] && G.T[1] <= 65535 && (G.T[0] + HG_TT - 1) / HG_TT <= 65535)
+    k_ref_to_planes_tiled<<<dim3((G.T[2] + HG_TT - 1) / HG_TT, (G.T[0] + HG_TT - 1) / HG_TT, G.T[1]),
+                            dim3(HG_TT, 8), 0, s>>>(G, ref, NT1, NT2, out);
+  else
+    k_ref_to_planes<<<L.grid_flux, HG_BLK, 0, s>>>(G, ref, NT1, NT2, out);
   if (G.p32 && out == G.p) launch_to_f32(G, L.grid_upd, s, G.p);  // the state set from the host
 }
 
 void launch_planes_to_ref(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *in, int NT0, int NT1,
                           int NT2, double *ref)
 {
-  k_planes_to_ref<<<L.grid_flux, HG_BLK, 0, s>>>(G, in, NT0, NT1, NT2, ref);
+  if (!G.deg[0] && !G.deg[2] && NT1 <= 65535 && (G.T[0] + HG_TT - 1) / HG_TT <= 65535)
+    k_planes_to_ref_tiled<<<dim3((G.T[2] + HG_TT - 1) / HG_TT, (G.T[0] + HG_TT - 1) / HG_TT, NT1), dim3(HG_TT, 8), 0,
+                            s>>>(G, in, NT1, NT2, ref);
+  else
+    k_planes_to_ref<<<L.grid_flux, HG_BLK, 0, s>>>(G, in, NT0, NT1, NT2, ref);
 }
 
 // Fluxes of direction d from the resident primitives G.p (hg_face_flux).
