@@ -3,6 +3,7 @@
 // Owns the device-resident grid of one simulation, converts between the
 // reference's array layout (flattened p[i][j][k][l]) and the engine's
 // structure-of-arrays layout, and launches the step (hg_kernels.cu).
+#include <cuda.h>  // CUpointer_attribute (queried through the runtime's driver entry point)
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -11,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
@@ -57,6 +59,7 @@ struct hg_handle {
   cudaGraphExec_t step_exec = nullptr;  // step_graph instantiated for hg_step
   bool exec_stale = true;
   bool graph_dirty = true;           // the capture predates a change of the kernels' arguments
+  uint64_t capture_gen = 0;          // number of captures of step_graph so far (batches compare it)
   double *d_tot = nullptr;           // hg_get_totals: per-block partials and the result
   int batch_refs = 0;                // batches this grid belongs to
   long ntot_ref = 0;          // N1TOT*N2TOT*N3TOT of the reference layout
@@ -473,9 +476,30 @@ static cudaError_t run_workers(long nch, W work)
   return cudaSuccess;
 }
 
-// True if the whole range [p, p + bytes) lies in page-locked host memory
-// (cudaHostAlloc or cudaHostRegister): the DMA engines can then read or
-// write the caller's buffer directly, with no staging copy on the host.
+// cuPointerGetAttribute through the runtime's driver entry point (no link
+// against libcuda); null if the driver does not provide it.
+typedef CUresult (*hg_ptr_attr_fn)(void *, CUpointer_attribute, CUdeviceptr);
+static hg_ptr_attr_fn ptr_attr_fn()
+{
+  static hg_ptr_attr_fn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (hg_ptr_attr_fn)f;
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// True if the whole range [p, p + bytes) lies in ONE page-locked host
+// allocation (cudaHostAlloc or cudaHostRegister): the DMA engines can then
+// read or write the caller's buffer directly, with no staging copy on the
+// host.  Both ends must be page-locked and carry the same allocation id, so
+// a range spanning two page-locked allocations with pageable memory between
+// them takes the staged path.
 static bool host_pinned(const void *p, size_t bytes)
 {
   cudaPointerAttributes a, b;
@@ -484,7 +508,13 @@ static bool host_pinned(const void *p, size_t bytes)
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeHost && b.type == cudaMemoryTypeHost;
+  if (a.type != cudaMemoryTypeHost || b.type != cudaMemoryTypeHost) return false;
+  hg_ptr_attr_fn fn = ptr_attr_fn();
+  unsigned long long ida = 0, idb = 0;
+  if (!fn || fn(&ida, CU_POINTER_ATTRIBUTE_BUFFER_ID, (CUdeviceptr)p) != CUDA_SUCCESS ||
+      fn(&idb, CU_POINTER_ATTRIBUTE_BUFFER_ID, (CUdeviceptr)((const char *)p + bytes - 1)) != CUDA_SUCCESS)
+    return false;
+  return ida == idb;
 }
 
 // FILL(dst, first zone, zones) writes that many zones of the reference order;
@@ -899,6 +929,7 @@ struct hg_batch {
   cudaStream_t stream = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool dirty = true;
+  std::vector<uint64_t> gens;       // each member's capture_gen when the batch graph was built
   hg::DevScalars **d_sc = nullptr;  // device array of the members' DevScalars pointers
   double *d_out = nullptr;          // 3 doubles per member: t, dt, err
   double *h_out = nullptr;          // pinned copy
@@ -921,6 +952,7 @@ static int capture_step(hg_handle *h)
   h->step_graph = g;
   h->graph_dirty = false;
   h->exec_stale = true;
+  h->capture_gen++;
   return HG_OK;
 }
 
@@ -936,10 +968,12 @@ static int batch_rebuild(hg_batch *b)
     return HG_OK;
   }
   std::vector<hg::DevScalars *> sc(n);
+  b->gens.assign(n, 0);
   for (int m = 0; m < n; m++) {
     int rc = capture_step(b->members[m]);
     if (rc != HG_OK) return rc;
     sc[m] = b->members[m]->G.sc;
+    b->gens[m] = b->members[m]->capture_gen;
   }
   HG_CK(cudaSetDevice(b->device));
   HG_CK(cudaMemcpyAsync(b->d_sc, sc.data(), sizeof(void *) * n, cudaMemcpyHostToDevice, b->stream));
@@ -1023,8 +1057,12 @@ extern "C" int hg_batch_step(hg_batch *b, double *t, double *dt)
 {
   if (!b) return HG_ERR_BADARG;
   HG_CK(cudaSetDevice(b->device));
-  for (hg_handle *m : b->members)
-    if (m->graph_dirty) b->dirty = true;
+  // A member recaptured since the batch graph was built (a solo hg_step after
+  // hg_set_geometry, hg_set_launch_config, hg_read_rdump, ...) holds new
+  // kernel arguments that the batch's copy of its old graph lacks.
+  for (size_t m = 0; m < b->members.size(); m++)
+    if (b->members[m]->graph_dirty || m >= b->gens.size() || b->gens[m] != b->members[m]->capture_gen)
+      b->dirty = true;
   if (b->dirty) {
     int rc = batch_rebuild(b);
     if (rc != HG_OK) return rc;

@@ -1632,14 +1632,16 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
 // every GPU that loads the library holds it (256 KiB + 256 B) until exit.
 // Host code never dereferences hg_na_scratch: it is a host-side stand-in for
 // the symbol, and a kernel given its host address would fault or read the
-// wrong memory.  The device address is looked up once per device with
-// cudaGetSymbolAddress on the first call made with that device current.
+// wrong memory.  Its device address comes from cudaGetSymbolAddress with the
+// device current: looked up again on every call made outside stream capture
+// (so a cudaDeviceReset, which reloads the module at a new address, is
+// followed), and taken from the last lookup on that device during capture.
 // ===========================================================================
 namespace hg {
 
 #define HG_NA_MAX_BLOCKS 32768  // one block per 128 faces: at most 4,194,304 faces per call
 static __device__ __align__(256) unsigned long long hg_na_scratch[HG_NA_MAX_BLOCKS + 32];
-static unsigned long long *hg_na_dev_ptr[64];  // device address of hg_na_scratch, per device ordinal
+static unsigned long long *hg_na_dev_ptr[64];  // last looked-up device address of hg_na_scratch, per device
 
 // face_flux() without the failure bookkeeping (the caller gets fluxes only).
 __device__ __forceinline__ double face_flux_na(const GridDev &G, const double *pl, const double *pr, const Geom &g,
@@ -1676,7 +1678,8 @@ __global__ void __launch_bounds__(HG_BLK) k_flux_noalloc(const __grid_constant__
                                                          int n0, int n1, int n2, double *max_out,
                                                          unsigned long long *scratch)
 {
-  const unsigned total = (unsigned)n0 * n1 * n2;  // < 2^31 (hg_init)
+  // total <= HG_NA_MAX_BLOCKS * HG_BLK faces: the entry point rejects larger calls
+  const unsigned total = (unsigned)n0 * n1 * n2;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double vmax = 0.;
   if (t < total) {
@@ -1765,10 +1768,15 @@ extern "C" int hg_face_flux_noalloc(const hg_grid_desc *d, const double *geom, c
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HG_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return HG_ERR_CUDA;
+  unsigned long long *scratch = nullptr;
   {
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
-    if (!hg_na_dev_ptr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone || !hg_na_dev_ptr[dev]) {
+      // the address of the array on the current device (allocates nothing)
       void *p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, hg_na_scratch);
       if (e != cudaSuccess || !p) {
@@ -1777,8 +1785,8 @@ extern "C" int hg_face_flux_noalloc(const hg_grid_desc *d, const double *geom, c
       }
       hg_na_dev_ptr[dev] = (unsigned long long *)p;
     }
+    scratch = hg_na_dev_ptr[dev];
   }
-  unsigned long long *scratch = hg_na_dev_ptr[dev];
   // the reference layout: variable innermost, k, j, i outermost
   GridDev G;
   memset(&G, 0, sizeof(G));
@@ -1804,7 +1812,6 @@ extern "C" int hg_face_flux_noalloc(const hg_grid_desc *d, const double *geom, c
   g.alpha = geom[34];
   for (int a = 0; a < 3; a++) g.beta[a] = geom[35 + a];
   for (int a = 0; a < 4; a++) g.ncon[a] = geom[38 + a];
-  cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemsetAsync(scratch + HG_NA_MAX_BLOCKS, 0, sizeof(unsigned long long), s) != cudaSuccess)
     return HG_ERR_CUDA;
   if (dir == 0)

@@ -140,9 +140,12 @@ int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max_char_speed
  * 4,194,304 faces in direction dir (HG_ERR_BADARG beyond).  Its scratch is a
  * 256 KiB array inside the library, held on every device that loads the
  * library until exit and shared by all calls: calls that overlap on the GPU
- * (e.g. on two streams) race and must be serialised by the caller.  The
- * first call on a device looks up that array's device address, so make the
- * first call on each device before any stream capture begins. */
+ * (e.g. on two streams) race and must be serialised by the caller.  A call
+ * made outside stream capture looks up that array's device address on the
+ * current device (allocating nothing); a call made while `stream` is being
+ * captured reuses the address of the last such lookup on that device, so
+ * make one call on each device before any stream capture begins (and again
+ * after a cudaDeviceReset). */
 int hg_face_flux_noalloc(const hg_grid_desc *desc, const double *geom, const double *prims, double *flux,
                          double *max_char_speed, int32_t dir, void *stream);
 

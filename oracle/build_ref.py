@@ -21,7 +21,8 @@ What it does, per configuration:
      dumps state and optionally loads an initial state (see ref_probe.c).
 
 Usage:  python oracle/build_ref.py [cfg ...]   (default: all configs)
-The reference tree is read from $HARM_REF_SRC or /root/reference/src.
+The reference tree is read from $HARM_REF_SRC, else from a checkout named
+`reference` beside this repository (<repo>/../reference/src).
 """
 import os
 import re
@@ -31,7 +32,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF_SRC = os.environ.get("HARM_REF_SRC", "/root/reference/src")
+REPO = os.path.dirname(HERE)
+REF_SRC = os.environ.get("HARM_REF_SRC") or os.path.join(os.path.dirname(REPO), "reference", "src")
 
 # src/makefile:364-373, minus corona.c corona2.c (cooling choices 4/5 only)
 # and minus the init file (one init.*.c is linked per configuration).

@@ -1,8 +1,8 @@
 /* harm_oracle.c -- CPU restatement of the HARM3D step (TEST INFRASTRUCTURE).
  *
- * The oracle: only tests/, __graft_entry__.smoke() and bench.py's
- * cpu_baseline leg load it, to verify the engine's results.  The product
- * never does.
+ * The oracle: only tests/ and __graft_entry__.smoke() load it, to verify
+ * the engine's results.  The product never does (bench.py's CPU baseline
+ * runs the reference's own build in oracle/_ref instead).
  *
  * It restates, loop by loop and in the same floating-point evaluation order,
  * the reference's time step of scnastro/coolharm3d (paths below are relative

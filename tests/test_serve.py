@@ -62,3 +62,48 @@ def test_server_results_same_alone_and_in_mix():
         assert a.checksum == s.checksum
     summ = serve.summarize(batched)
     assert summ["requests"] == 10 and summ["p99_s"] >= summ["p50_s"] > 0
+
+
+def _scaled_minkowski(geom, s):
+    """Minkowski space in coordinates stretched by s: gcov = diag(-1, s^2, s^2, s^2)."""
+    g = geom.copy()
+    gcon, gcov = g[:16].reshape(4, 4), g[16:32].reshape(4, 4)
+    for a in (1, 2, 3):
+        gcov[a, a] = s * s
+        gcon[a, a] = 1.0 / (s * s)
+    g[32], g[33] = s ** 3, 1.0 / s ** 3
+    return g
+
+
+def test_member_changed_and_stepped_alone_is_recaptured_in_batch():
+    """A member whose kernel arguments change (new geometry) and which then
+    takes a step alone (recapturing its own step graph) must not be advanced
+    by the batch's copy of its old graph: the batch rebuilds when a member's
+    capture generation moved on."""
+    prob = setups.linear_wave((12, 12, 12))
+    geom0, _ = hg.minkowski_tables(prob.desc)
+    geom1 = _scaled_minkowski(geom0, 1.1)
+    a = hg.Engine(prob.desc)
+    setups.start(a, prob)
+    other = hg.Engine(setups.balsara1(64).desc)
+    setups.start(other, setups.balsara1(64))
+    b = hg.Batch(0, 4)
+    b.add(a)
+    b.add(other)
+    for _ in range(3):
+        b.step()
+    a.set_geometry(geom1)
+    a.step(1)          # recaptures a's own step graph with geom1
+    for _ in range(2):
+        b.step()       # must run a with geom1 too
+    b.remove(a)
+    b.remove(other)
+    b.close()
+    ref = hg.Engine(prob.desc)
+    setups.start(ref, prob)
+    ref.step(3)
+    ref.set_geometry(geom1)
+    ref.step(3)
+    np.testing.assert_array_equal(a.download(), ref.download())
+    for e in (a, other, ref):
+        e.close()

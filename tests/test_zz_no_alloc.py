@@ -4,8 +4,9 @@ that owns the device, or in loops that cannot afford cudaMalloc's
 synchronisation).  Its only scratch is a static array inside the library.
 
 Checked through the C ABI against the allocating entry point hg_face_flux on
-two calls in a row (the second reuses the scratch the first left behind);
-both must agree bit for bit, the tolerance of the FP64 parity tests.  This
+three calls in a row (each reuses the scratch the one before left behind),
+covering the HLL and the LF flux and all three directions; both must agree
+bit for bit, the tolerance of the FP64 parity tests.  This
 file sorts last so that a run stopping at the first failure has run every
 other test first."""
 import ctypes
@@ -31,13 +32,15 @@ def _engine(f):
     return d, geom, e
 
 
-def test_noalloc_flux_matches_allocating_entry_point_on_two_calls():
+def test_noalloc_flux_matches_allocating_entry_point_on_consecutive_calls():
     import torch
     lib = hg.load_library()
-    calls = [("linwave_noee_stress_10x8x6_s2", 0), ("linwave_12x10x8_s2", 1)]
+    # HLL (PPM_MC) along x1 and x2, then LF (PPM_VL) along x3
+    calls = [("linwave_noee_stress_10x8x6_s2", 0), ("linwave_12x10x8_s2", 1), ("linwave_vl_stress_8x8x8_s2", 2)]
     stream = torch.cuda.current_stream()
     for name, d in calls:
         f = fixtures.load(name)
+        assert f["sw"]["flux"] == (0 if "_vl_" in name else 1)
         desc, geom, e = _engine(f)
         want, want_max = e.face_flux(d)
         prims = torch.from_numpy(np.ascontiguousarray(f["p0"])).cuda()
