@@ -21,7 +21,7 @@ NG, NP, NFAIL, NGEOM = 3, 8, 15, 42
 RECON_MINMOD, RECON_VANL, RECON_MC, RECON_PPM_MM, RECON_PPM_VL, RECON_PPM_MC = range(6)
 FLUX_LF, FLUX_HLLE = 0, 1
 BC_CARTESIAN_OUTFLOW, BC_CARTESIAN_PERIODIC, BC_SPHERICAL_OUTFLOW3 = 0, 1, 10
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP64_FMA = 0, 1, 2
 
 # nfail[] slots (macros.h:243-258)
 NFAIL_NAMES = ["FLOOR", "TMAX", "GAMMA_MAX", "GAMMA_CALC", "USE_FULL_INV", "USE_EE", "UTOPRIM",

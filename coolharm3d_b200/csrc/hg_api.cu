@@ -37,6 +37,21 @@ void launch_planes_to_ref(const GridDev &G, const LaunchCfg &L, cudaStream_t s, 
                           int NT2, double *ref);
 }  // namespace hg
 
+// The same step kernels built with contracted multiply-adds
+// (hg_kernels.cu compiled with HG_FMA_BUILD): HG_PREC_FP64_FMA.
+namespace hg_fma {
+void launch_step(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s, hg::EventRec *R);
+void launch_face_flux(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s, int d);
+cudaError_t prepare_kernels();
+}  // namespace hg_fma
+
+// one step's launch sequence of the grid's precision form
+static void launch_grid_step(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s, hg::EventRec *R)
+{
+  if (G.prec == HG_PREC_FP64_FMA) hg_fma::launch_step(G, L, s, R);
+  else hg::launch_step(G, L, s, R);
+}
+
 using hg::GridDev;
 
 #define HG_XCH_THREADS 8              // host threads of one transfer
@@ -140,7 +155,8 @@ static int validate(const hg_grid_desc *d)
   if (d->bc_type == 10 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
   if (d->metric_dim != 0 && d->metric_dim != 2) return HG_ERR_BADARG;
   if (d->cooling != 0 && d->cooling != 1) return HG_ERR_BADARG;
-  if (d->precision != HG_PREC_FP64 && d->precision != HG_PREC_MIXED) return HG_ERR_BADARG;
+  if (d->precision != HG_PREC_FP64 && d->precision != HG_PREC_MIXED && d->precision != HG_PREC_FP64_FMA)
+    return HG_ERR_BADARG;
   // the tables of METRIC_DIM 2 vary with i and j: those directions must be resolved
   if (d->metric_dim == 2 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
   if (d->rescale_r && d->n1 == 1) return HG_ERR_BADARG;
@@ -203,7 +219,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     if ((rc = dev_alloc(h, &q_, (bytes))) != HG_OK) goto fail; \
     ptr = (decltype(ptr))q_;                                  \
   } while (0)
-  if (hg::prepare_kernels() != cudaSuccess ||
+  if (hg::prepare_kernels() != cudaSuccess || hg_fma::prepare_kernels() != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     delete h;
@@ -713,7 +729,7 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
   }
   HG_CK(cudaEventRecord(h->ev0, h->stream));
   for (int s = 0; s < nsteps; s++) {
-    if (R) hg::launch_step(h->G, h->L, h->stream, R);
+    if (R) launch_grid_step(h->G, h->L, h->stream, R);
     else HG_CK(cudaGraphLaunch(h->step_exec, h->stream));
   }
   HG_CK(cudaGetLastError());
@@ -757,7 +773,8 @@ extern "C" int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
   HG_CK(cudaMemsetAsync(G.F[dir], 0, sizeof(double) * HG_NPR * G.S, h->stream));
-  hg::launch_face_flux(G, h->L, h->stream, dir);
+  if (G.prec == HG_PREC_FP64_FMA) hg_fma::launch_face_flux(G, h->L, h->stream, dir);
+  else hg::launch_face_flux(G, h->L, h->stream, dir);
   HG_CK(cudaGetLastError());
   HG_CK(cudaStreamSynchronize(h->stream));
   // per-cell planes -> reference layout with the variable index innermost
@@ -944,7 +961,7 @@ static int capture_step(hg_handle *h)
   }
   HG_CK(cudaSetDevice(h->d.device));
   HG_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  hg::launch_step(h->G, h->L, h->stream, nullptr);
+  launch_grid_step(h->G, h->L, h->stream, nullptr);
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
   HG_CK(e);

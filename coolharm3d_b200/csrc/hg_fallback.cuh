@@ -2,14 +2,16 @@
 // Utoprim_1d, the entropy-equation fix with Utoprim_1d_ee / Utoprim_1d_ee2,
 // run by the fallback kernel over a compacted queue of zones whose 2D Newton
 // inversion failed or that need the entropy fix.  Same operation order as the
-// reference routines named beside each function.
+// reference routines named beside each function.  Every power of the density
+// goes through hg_cr_pow (correctly rounded, hg_crpow.h) instead of pow().
 #pragma once
+#include "hg_crpow.h"
 #include "hg_phys.cuh"
 
 namespace hg {
 
 // Utoprim_1d (utoprim_1d.c:118-629)
-__device__ __noinline__ int utoprim_1d(const double *U, const Geom &g, double gam, double *prim, double *gamma_out,
+static __device__ __noinline__ int utoprim_1d(const double *U, const Geom &g, double gam, double *prim, double *gamma_out,
                                        double *bsq_out)
 {
   double Ut[HG_NPR], pt[HG_NPR];
@@ -130,14 +132,14 @@ struct EEState {
   double t2, t4, t7, t24, t300, t400, s100, s200;
 };
 
-__device__ __noinline__ int ee_gnr2(EEState &s, double *x)  // gnr2 + func_rho (utoprim_1d_ee.c:640-847)
+static __device__ __noinline__ int ee_gnr2(EEState &s, double *x)  // gnr2 + func_rho (utoprim_1d_ee.c:640-847)
 {
   double f = 1., df = 1., errx = 1.;
   int n_iter = 0, i_extra = 0, doing_extra = 0;
   bool keep = true;
   while (keep) {
     const double rho = x[0], W = s.W_for_gnr2;
-    const double t40 = pow(rho, s.gm1);
+    const double t40 = hg_cr_pow(rho, s.gm1);
     s.rho_gm1 = t40;
     const double resid = (rho * W + (-t40 * s.s100 - s.D) * s.D);
     const double t14 = t40 / rho;
@@ -161,7 +163,7 @@ __device__ __noinline__ int ee_gnr2(EEState &s, double *x)  // gnr2 + func_rho (
   return 1;
 }
 
-__device__ __noinline__ int ee_gnr(EEState &s, double *x)  // general_newton_raphson + func_W
+static __device__ __noinline__ int ee_gnr(EEState &s, double *x)  // general_newton_raphson + func_W
 {
   double f = 1., df = 1., errx = 1.;
   int n_iter = 0, i_extra = 0, doing_extra = 0;
@@ -179,7 +181,7 @@ __device__ __noinline__ int ee_gnr(EEState &s, double *x)  // general_newton_rap
     }
     s.rho_for_gnr2_old = s.rho_for_gnr2;
     const double rho = s.rho_for_gnr2 = x_rho[0];
-    s.rho_gm1 = pow(rho, s.gm1);
+    s.rho_gm1 = hg_cr_pow(rho, s.gm1);
     s.drho_dW = -rho * rho / (-s.rho_gm1 * s.s200 + W * rho);
     const double t15 = -(s.D - rho) * (s.D + rho);
     const double t200 = W + s.two_Bsq;
@@ -207,7 +209,7 @@ __device__ __noinline__ int ee_gnr(EEState &s, double *x)  // general_newton_rap
   return 1;
 }
 
-__device__ __noinline__ int utoprim_1d_ee(const double *U, double S, const Geom &g, double gam, double *prim,
+static __device__ __noinline__ int utoprim_1d_ee(const double *U, double S, const Geom &g, double gam, double *prim,
                                           double *gamma_out)
 {
   if (U[0] <= 0.) return -100;
@@ -247,7 +249,7 @@ __device__ __noinline__ int utoprim_1d_ee(const double *U, double S, const Geom 
   const double gammasq = 1. + utsq;
   double gamma = sqrt(gammasq);
   double rho0 = s.D / gamma;
-  s.rho_gm1 = pow(rho0, s.gm1);
+  s.rho_gm1 = hg_cr_pow(rho0, s.gm1);
   double p = s.Sc * s.rho_gm1 / gamma;
   double u = p * s.gm1_inv;
   double w = rho0 + u + p;
@@ -276,7 +278,7 @@ __device__ __noinline__ int utoprim_1d_ee(const double *U, double S, const Geom 
   s.rho_for_gnr2 = x_rho[0];
   if (retval != 0) return 10;
   rho0 = s.rho_for_gnr2;
-  s.rho_gm1 = pow(rho0, s.gm1);
+  s.rho_gm1 = hg_cr_pow(rho0, s.gm1);
   utsq = (s.D - rho0) * (s.D + rho0) / (rho0 * rho0);
   const double gamma_sq = 1. + utsq;
   gamma = sqrt(gamma_sq);
@@ -295,7 +297,7 @@ __device__ __noinline__ int utoprim_1d_ee(const double *U, double S, const Geom 
 }
 
 // Utoprim_1d_ee2 (utoprim_1d_ee2.c:152-590): one Newton iteration in rho.
-__device__ __noinline__ int utoprim_1d_ee2(const double *U, double S, const Geom &g, double gam, double *prim,
+static __device__ __noinline__ int utoprim_1d_ee2(const double *U, double S, const Geom &g, double gam, double *prim,
                                            double *gamma_out)
 {
   if (U[0] <= 0.) return -100;
@@ -332,7 +334,7 @@ __device__ __noinline__ int utoprim_1d_ee2(const double *U, double S, const Geom
     // func_rho (utoprim_1d_ee2.c:540-585)
     const double rho = x, rhosq = rho * rho;
     const double t200 = 1. / (D * D);
-    const double t100 = g_o_gm1 * Sc * pow(rho, (gam - 1.));
+    const double t100 = g_o_gm1 * Sc * hg_cr_pow(rho, (gam - 1.));
     const double W = D * (D + t100) / rho;
     const double dWdrho = D * (-D + t100 * (gam - 2.)) / rhosq;
     const double t1 = W * W, t2 = Bsq + W, t3 = t2 * t2;
@@ -369,7 +371,7 @@ __device__ __noinline__ int utoprim_1d_ee2(const double *U, double S, const Geom
   gamma = sqrt(gamma_sq);
   *gamma_out = gamma;
   if (utsq < 0.) return 4;
-  const double rho_gm1 = pow(rho0, (gam - 1.));
+  const double rho_gm1 = hg_cr_pow(rho0, (gam - 1.));
   const double p = Sc * rho_gm1 / gamma;
   const double u = p / (gam - 1.);
   const double w = rho0 + u + p;

@@ -28,7 +28,28 @@
 #include "hg_common.cuh"
 #include "hg_fallback.cuh"
 
+// This file is compiled twice.  Plain: into namespace hg with no multiply-add
+// contracted (-fmad=false), every FP64 operation rounded as in the
+// reference's build (HG_PREC_FP64, bit-identical results).  With HG_FMA_BUILD
+// and -fmad=true: the same kernels and launch sequence into namespace hg_fma,
+// where the compiler fuses multiply-adds (HG_PREC_FP64_FMA: fewer FP64
+// instructions, results within rounding of the plain form).  Types and the
+// device functions of the headers are shared through namespace hg.
+#ifdef HG_FMA_BUILD
+#define HG_KNS hg_fma
+#else
+#define HG_KNS hg
+#endif
+
 namespace hg {
+// the FP32 flux kernels of the mixed form (hg_mixed.cu)
+void launch_flux_f32(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d, const int *lo, const int *n,
+                     unsigned int mult);
+void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
+}  // namespace hg
+
+namespace HG_KNS {
+using namespace hg;
 
 // register caps of the two update kernels (4 blocks of 128 threads per SM;
 // measured best of 1-6 blocks on the torus)
@@ -634,7 +655,8 @@ __global__ void __launch_bounds__(HG_BLK, HG_C2P_MINB) k_update_c2p(const __grid
 // ---------------------------------------------------------------------------
 // fixup_entropy_eq(), fixup.c:335-454: entropy flux rebuilt from the face
 // states of the six faces (recomputed here; the flux kernel does not store
-// them) and the inversions Utoprim_1d_ee / Utoprim_1d_ee2.
+// them) and the inversions Utoprim_1d_ee / Utoprim_1d_ee2.  pow() of the
+// reference is the correctly rounded hg_cr_pow (hg_crpow.h).
 template <bool RS>
 __device__ __forceinline__ double ee_face_flux(const GridDev &G, const double *p_h, int d, int i, int j, int k)
 {
@@ -655,10 +677,10 @@ __device__ __forceinline__ double ee_face_flux(const GridDev &G, const double *p
   const double cmin = fabs(a1 > -cminr ? a1 : -cminr);
   const double ctop = cmin > cmax ? cmin : cmax;
   const double gam = G.gam;
-  double s = (gam - 1.) * pl[UU] * pow(pl[RHO], 1. - gam);
+  double s = (gam - 1.) * pl[UU] * hg_cr_pow(pl[RHO], 1. - gam);
   const double Ul = s * (g.g * ql.ucon[0]);
   const double Fl = s * (g.g * ql.ucon[dim]);
-  s = (gam - 1.) * pr[UU] * pow(pr[RHO], 1. - gam);
+  s = (gam - 1.) * pr[UU] * hg_cr_pow(pr[RHO], 1. - gam);
   const double Ur = s * (g.g * qr.ucon[0]);
   const double Fr = s * (g.g * qr.ucon[dim]);
   if (G.flux == 1) return (cmax * Fl + cmin * Fr - cmax * cmin * (Ur - Ul)) / (cmax + cmin + HG_SMALL);
@@ -690,7 +712,7 @@ __device__ __noinline__ int fixup_entropy_eq(const GridDev &G, long e, int i, in
   for (int l = 0; l < HG_NPR; l++) prim_backup[l] = prim[l];
   const double gam = G.gam;
   gamma_calc(prim_old, geom, &gamma);
-  const double S_old = geom.g * (gam - 1.) * prim_old[UU] * gamma / (geom.alpha * pow(prim_old[RHO], (gam - 1.)));
+  const double S_old = geom.g * (gam - 1.) * prim_old[UU] * gamma / (geom.alpha * hg_cr_pow(prim_old[RHO], (gam - 1.)));
   double Fm[3], Fp[3];
   for (int d = 0; d < 3; d++) {
     Fm[d] = G.q_F[6 * e + d];
@@ -1170,10 +1192,6 @@ static inline void mark(EventRec *r, int cls, cudaStream_t s)
   r->n++;
 }
 
-void launch_flux_f32(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d, const int *lo, const int *n,
-                     unsigned int mult);
-void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
-
 // k_flux_strip keeps 16 * NF face states per thread in dynamic shared memory
 // (16, 32 and 48 KiB per block for NF = 1, 2, 3; the limit is raised once
 // per instantiation).  Longer strips save reconstruction work but their
@@ -1623,7 +1641,9 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
   mark(R, KC_END, s);
 }
 
-}  // namespace hg
+}  // namespace HG_KNS
+
+#ifndef HG_FMA_BUILD
 
 // ===========================================================================
 // hg_face_flux_noalloc: hg_face_flux for callers that cannot allocate device
@@ -1830,3 +1850,5 @@ extern "C" int hg_face_flux_noalloc(const hg_grid_desc *d, const double *geom, c
   }
   return HG_OK;
 }
+
+#endif  // HG_FMA_BUILD

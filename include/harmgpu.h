@@ -45,6 +45,8 @@ extern "C" {
 
 #define HG_PREC_FP64 0          /* every operation in IEEE double, no FMA: bit-identical to the reference */
 #define HG_PREC_MIXED 1         /* reconstruction + HLL flux in FP32, everything else FP64 */
+#define HG_PREC_FP64_FMA 2      /* every operation in IEEE double, multiply-adds fused: within
+                                   rounding of HG_PREC_FP64, not bit-identical */
 
 /* Run description: the options.h switches of the path plus init_base() values. */
 typedef struct hg_grid_desc {

@@ -14,6 +14,9 @@
  *   HARM_PROBE_MAXSTEPS=N      stop (exit 0) after N steps
  *   HARM_PROBE_TIME=1          print one line "probe_time steps=<n> seconds=<s>
  *                              cells=<NCELLS>" timing only the step calls
+ *   HARM_PROBE_FINAL=1         write <prefix>.<nstep>.bin after the step that
+ *                              reaches t >= GridLength[0] (where main()'s loop,
+ *                              main.c:64, ends the run) and exit 0
  *
  * State file (native little-endian):
  *   char magic[4]="HGST"; int32 version=1;
@@ -202,6 +205,14 @@ void step_ch(void)
   /* main() increments nstep after this returns; report the step count done */
   int done = nstep + 1;
   int last = (probe_maxsteps > 0 && probe_steps >= probe_maxsteps);
+  if (getenv("HARM_PROBE_FINAL") && t >= GridLength[0]) {
+    int save = nstep;
+    nstep = done;
+    dump_state(done);
+    nstep = save;
+    probe_finish();
+    exit(0);
+  }
   if (should_dump(done) || (last && getenv("HARM_PROBE_OUT") && !getenv("HARM_PROBE_DUMP"))) {
     int save = nstep;
     nstep = done;

@@ -5,6 +5,9 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# runs long enough that the reference's own last-bit sensitivity is O(1e-4):
+# compared in tests/test_t_final.py against the stored correctly rounded run
+CHAOTIC = {"torus_24x16x8_s200"}
 
 
 def names():

@@ -47,7 +47,31 @@ CASES = [
     ("torus_stress_16x24x6_s1", "torus", (16, 24, 6), 1, 23),
     # advected field loop, 2D periodic: the reference's own initial data
     ("field_loop_24x24x1_s3", "field_loop", (24, 24, 1), 3, None),
+    # whole runs: the reference's own initial data run to its own final time
+    # (GridLength[0]): Balsara-1 to t = 0.4, one period of the 2D slow wave;
+    # and 200 steps of the small torus
+    ("balsara1_n1024_tfinal", "balsara1", (1024, 1, 1), "final", None),
+    ("linwave_2d_32x32x1_tfinal", "linwave", (32, 32, 1), "final", None),
+    ("torus_24x16x8_s200", "torus", (24, 16, 8), 200, "load"),
 ]
+
+# Runs long enough for the flow to amplify a one-ulp change of pow() to O(1):
+# besides the reference's result they hold the reference's algorithm run by
+# the C oracle (pinned bit for bit to the reference build) with the engine's
+# correctly rounded pow() ("cr_*": the result the engine must reproduce) and
+# with glibc's pow() moved up one ulp ("ulp_p": the reference's own
+# sensitivity to the last bit of pow()).
+CHAOTIC = {"torus_24x16x8_s200"}
+
+
+def oracle_run(lib, out, steps):
+    o = ht.Oracle(tuple(int(x) for x in out["n"]), ht.CONFIG_SWITCHES[out["config"]],
+                  dict(gam=out["gam"], cour=out["cour"], grid_length=out["grid_length"], startx=out["startx"],
+                       dx=out["dx"], geom=out["geom"], conn=out["conn"], cell6=out["cell6_full"],
+                       rface=out["rface"], cool_omega=out["cool_omega"], cool_temp=out["cool_temp"]), lib=lib)
+    o.set_state(out["p0"], out["t0"], out["dt0"])
+    o.step(steps)
+    return o.state()
 
 
 def stress_state(p, seed):
@@ -97,8 +121,12 @@ def make(name, cfg, n, steps, seed):
         p0 = stress_state(s0["p"], seed)
         t0, dt0 = s0["t"], 1e-4
         load = dict(p=p0, t=t0, dt=dt0)
-    r = ht.run_ref(cfg, n, steps, load=load)
-    s = r["states"][steps]
+    if steps == "final":
+        s, _ = ht.run_ref_final(cfg, n, load=load)
+        steps = s["nstep"]
+    else:
+        r = ht.run_ref(cfg, n, steps, load=load)
+        s = r["states"][steps]
     sw = ht.CONFIG_SWITCHES[cfg]
     out = dict(
         config=cfg, n=np.array(n), steps=steps, p0=p0, t0=t0, dt0=dt0,
@@ -114,6 +142,13 @@ def make(name, cfg, n, steps, seed):
     out["rface"] = geom["rface"]
     out["cool_omega"] = geom["cool_omega"]
     out["cool_temp"] = geom["cool_temp"]
+    if name in CHAOTIC:
+        out["cell6_full"] = geom["cell6"]
+        c = oracle_run(ht.CR_ORACLE, out, steps)
+        for k in ("p", "pflag", "gamma", "nfail", "nfailtot", "t", "dt", "m_tot"):
+            out["cr_" + k] = c[k]
+        out["ulp_p"] = oracle_run("liboracle_powulp.so", out, steps)["p"]
+        del out["cell6_full"]
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(name, "nfailtot", s["nfailtot"].tolist())
 

@@ -122,6 +122,32 @@ def run_ref(cfg, n, steps, load=None, dumps=(), want_geom=False, timeout=600):
     return dict(states=states, geom=geom)
 
 
+def run_ref_final(cfg, n, load=None, want_geom=False, timeout=3600):
+    """Run the reference build `cfg` until its own final time GridLength[0]
+    (main.c:64) and return (state at t_final, geometry-or-None)."""
+    with tempfile.TemporaryDirectory() as td:
+        env = dict(os.environ)
+        env["HARM_PROBE_OUT"] = os.path.join(td, "st")
+        env["HARM_PROBE_FINAL"] = "1"
+        env.pop("HARM_PROBE_MAXSTEPS", None)
+        env.pop("HARM_PROBE_DUMP", None)
+        if want_geom:
+            env["HARM_PROBE_GEOM"] = os.path.join(td, "geom.bin")
+        if load is not None:
+            lp = os.path.join(td, "load.bin")
+            write_state(lp, load["p"], load["t"], load["dt"])
+            env["HARM_PROBE_LOAD"] = lp
+        r = subprocess.run([str(ref_exe(cfg)), "1", "1", "1"] + [str(x) for x in n], cwd=td, env=env,
+                           stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError("reference run failed: %s\n%s" % (r.returncode, r.stderr[-2000:]))
+        files = sorted(Path(td).glob("st.*.bin"))
+        assert len(files) == 1, files
+        state = read_state(files[0])
+        geom = read_geom(os.path.join(td, "geom.bin"), n) if want_geom else None
+    return state, geom
+
+
 class OrDesc(ctypes.Structure):
     _fields_ = [("n1", ctypes.c_int32), ("n2", ctypes.c_int32), ("n3", ctypes.c_int32),
                 ("recon_type", ctypes.c_int32), ("flux_type", ctypes.c_int32),
@@ -134,31 +160,53 @@ class OrDesc(ctypes.Structure):
 
 
 _olib = None
+_olibs = {}
+# The oracle builds (oracle/Makefile): "liboracle.so" with glibc's pow() (the
+# reference's own arithmetic), "liboracle_cr.so" with the correctly rounded
+# pow() the engine uses, "liboracle_powcmp.so" glibc's pow() counting where
+# the two differ.
+CR_ORACLE = "liboracle_cr.so"
 
 
-def oracle_lib():
+def ensure_oracle(name="liboracle.so"):
+    """Path of an oracle build, made with oracle/Makefile if missing."""
+    path = REPO / "oracle" / name
+    if not path.exists():
+        subprocess.check_call(["make", "-s", "-C", str(REPO / "oracle"), name])
+    return path
+
+
+def oracle_lib(name=None):
+    """The oracle library: the one at ORACLE_SO, or the build `name`."""
     global _olib
+    if name is not None:
+        if name not in _olibs:
+            _olibs[name] = _configure(ctypes.CDLL(str(ensure_oracle(name))))
+        return _olibs[name]
     if _olib is None:
         if not ORACLE_SO.exists():
             subprocess.check_call(["make", "-s", "-C", str(REPO / "oracle"), "liboracle.so"])
-        lib = ctypes.CDLL(str(ORACLE_SO))
-        P = ctypes.c_void_p
-        lib.or_create.restype = P
-        lib.or_create.argtypes = [ctypes.POINTER(OrDesc), P, P, P, P]
-        lib.or_destroy.argtypes = [P]
-        lib.or_set_prims.argtypes = [P, P, ctypes.c_double, ctypes.c_double]
-        for fn in ("or_get_prims", "or_get_pflag", "or_get_gamma", "or_get_nfail", "or_get_nfailtot"):
-            getattr(lib, fn).argtypes = [P, P]
-        lib.or_get_time.argtypes = [P, P, P, P]
-        lib.or_step.argtypes = [P, ctypes.c_int]
-        lib.or_fixup_bounds.argtypes = [P]
-        lib.or_totals.argtypes = [P, P, P, P]
-        lib.or_face_flux.argtypes = [P, ctypes.c_int, P, P]
-        lib.or_set_cooling.argtypes = [P, P, P]
-        lib.or_ntot.restype = ctypes.c_long
-        lib.or_ntot.argtypes = [P]
-        _olib = lib
+        _olib = _configure(ctypes.CDLL(str(ORACLE_SO)))
     return _olib
+
+
+def _configure(lib):
+    P = ctypes.c_void_p
+    lib.or_create.restype = P
+    lib.or_create.argtypes = [ctypes.POINTER(OrDesc), P, P, P, P]
+    lib.or_destroy.argtypes = [P]
+    lib.or_set_prims.argtypes = [P, P, ctypes.c_double, ctypes.c_double]
+    for fn in ("or_get_prims", "or_get_pflag", "or_get_gamma", "or_get_nfail", "or_get_nfailtot"):
+        getattr(lib, fn).argtypes = [P, P]
+    lib.or_get_time.argtypes = [P, P, P, P]
+    lib.or_step.argtypes = [P, ctypes.c_int]
+    lib.or_fixup_bounds.argtypes = [P]
+    lib.or_totals.argtypes = [P, P, P, P]
+    lib.or_face_flux.argtypes = [P, ctypes.c_int, P, P]
+    lib.or_set_cooling.argtypes = [P, P, P]
+    lib.or_ntot.restype = ctypes.c_long
+    lib.or_ntot.argtypes = [P]
+    return lib
 
 
 def _ptr(a):
@@ -166,10 +214,12 @@ def _ptr(a):
 
 
 class Oracle:
-    """The C restatement of the reference step (oracle/harm_oracle.c)."""
+    """The C restatement of the reference step (oracle/harm_oracle.c).
+    lib: which oracle build (None: ORACLE_SO, glibc's pow(); CR_ORACLE: the
+    correctly rounded pow() of the engine)."""
 
-    def __init__(self, n, sw, geomd):
-        self.lib = oracle_lib()
+    def __init__(self, n, sw, geomd, lib=None):
+        self.lib = oracle_lib(lib)
         d = OrDesc()
         d.n1, d.n2, d.n3 = n
         d.recon_type, d.flux_type, d.use_flux_ct_para = sw["recon"], sw["flux"], sw["ct_para"]

@@ -1,16 +1,16 @@
 """Parity at the benchmark's full size: the 192x192x128 magnetised torus
 (Kerr-Schild a = 0.9, cooling, PPM_MC, HLLE, entropy fix, RESCALE_R), one
 RK2 step of the engine against one step of the C oracle from the same
-state.  Same bar as the fixture tests: bit-identical primitives, pflag,
-p_gamma and counters, with zones repaired by the entropy fix held to the
-pow() tolerance (tests/test_gpu_parity.py)."""
+state (the build with the engine's correctly rounded pow(), see
+tests/test_gpu_parity.py): bit-identical primitives, pflag, p_gamma and
+counters in every zone, those repaired by the entropy fix included."""
 import numpy as np
 import pytest
 
 import coolharm3d_b200 as hg
 import harmtest as ht
 from coolharm3d_b200 import torus
-from test_gpu_parity import RTOL_POW, assert_same, uses_pow
+from test_gpu_parity import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +30,7 @@ def test_full_size_torus_step_matches_oracle():
     o = ht.Oracle(N, SW, dict(gam=d.gam, cour=d.cour, grid_length=np.array(d.grid_length[:]),
                                startx=np.array(d.startx[:]), dx=np.array(d.dx[:]), geom=t["geom"], conn=t["conn"],
                                cell6=t["cell6"], rface=t["rface"], cool_omega=t["cool_omega"],
-                               cool_temp=t["cool_temp"]))
+                               cool_temp=t["cool_temp"]), lib=ht.CR_ORACLE)
     o.set_state(p0, d.t, d.dx[0])
     e.set_time(d.t, d.dx[0])
     o.step(1)
@@ -38,5 +38,5 @@ def test_full_size_torus_step_matches_oracle():
     ref = o.state()
     ref["sw"] = SW
     assert (t1, dt1) == (ref["t"], ref["dt"])
-    assert_same(e, ref, N, rtol=RTOL_POW if uses_pow(ref) else 0.0)
+    assert_same(e, ref, N)
     e.close()

@@ -117,7 +117,7 @@ def _oracle(prob):
               ee=d.use_entropy_eq, cooling=0, rescale=0)
     geomd = dict(gam=d.gam, cour=d.cour, grid_length=np.array(d.grid_length[:]), startx=np.array(d.startx[:]),
                  dx=np.array(d.dx[:]), geom=prob.geom, conn=np.zeros(1), cell6=prob.cell6, rface=None)
-    return ht.Oracle(prob.n, sw, geomd)
+    return ht.Oracle(prob.n, sw, geomd, lib=ht.CR_ORACLE)
 
 
 @pytest.mark.gpu

@@ -4,10 +4,11 @@ pow() is correctly rounded neither in glibc nor in CUDA, and the entropy fix
 (fixup.c:335-454, utoprim_1d_ee.c, utoprim_1d_ee2.c) feeds pow() results
 into Newton solves.  This test rebuilds the C oracle with every pow() result
 moved up by one ulp and measures the change after one step on the stress
-fixtures: it is far above 1e-12, which is why zones repaired by the entropy
-fix are compared with a relative tolerance (1e-9 after one step) instead of
-bit for bit in tests/test_gpu_parity.py, while pflag and all failure
-counters must still agree exactly."""
+fixtures: it is far above 1e-12.  This is why the engine does not use the
+device's pow() there but hg_cr_pow, a correctly rounded pow() with the same
+bits on host and device (tests/test_crpow.py): with it the engine matches the
+reference bit for bit wherever glibc's pow() is correctly rounded, and pflag
+and all failure counters must still agree exactly."""
 import ctypes
 import os
 import subprocess

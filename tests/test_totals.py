@@ -14,7 +14,7 @@ CASES = ["linwave_noee_stress_10x8x6_s2", "linwave_12x10x8_s2", "balsara1_n128_s
 
 
 def oracle_after(f):
-    o = ht.Oracle(f["n"], f["sw"], fixtures.geomd(f))
+    o = ht.Oracle(f["n"], f["sw"], fixtures.geomd(f), lib=ht.CR_ORACLE)
     o.set_state(f["p0"], f["t0"], f["dt0"])
     o.step(f["steps"])
     return o
