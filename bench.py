@@ -23,11 +23,13 @@ Multi-GPU (torchrun): the path does not shard across GPUs in this engine
 ranks, value = total zone-updates of all ranks / that time ("weak").
 
 The reference arm (--impl reference) times the reference's own CPU build
-(oracle/_ref/<config>/harm3d, made from the reference sources by
-oracle/build_ref.py) on the host cores: one process per core, each running
-the same problem on the block one rank of a 4x4x4 decomposition would own
-(48x48x32 of the torus, 64^3 of the linear wave), without MPI (no halo
-exchange, so an upper bound on the MPI build's rate).
+(compiled on the host with gcc -O3 -march=native -fcommon from the sources
+oracle/build_ref.py staged in oracle/_ref/<config>/src) on the host cores:
+the workload's grid split into one block per core as the reference's MPI
+runs split it (192x192x128 over 16 cores: 2x2x4 blocks of 96x96x32), every
+block advanced by its own process for W untimed + K timed steps, without MPI
+(no halo exchange, so an upper bound on the MPI build's rate), plus one
+single-process step of the whole grid for the per-zone cost at full size.
 """
 import argparse
 import json
@@ -60,25 +62,27 @@ def parse():
                     help="steps per candidate of the launch-configuration autotuner (0: keep the defaults)")
     ap.add_argument("--mixed-steps", type=int, default=2000,
                     help="steps of the mixed-precision accuracy comparison (0: skip the mixed form)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma"],
+                    help="form timed for `value`: fp64 (bit-identical to the reference) or fp64_fma "
+                         "(fused multiply-adds)")
+    ap.add_argument("--fma-steps", type=int, default=200,
+                    help="steps of the FP64-with-FMA accuracy comparison beside the fp64 line (0: skip)")
     return ap.parse_args()
 
 
 WORKLOADS = {
-    "torus192": dict(kind="torus", n=(192, 192, 128), ref_cfg="torus", ref_block=(48, 48, 32),
+    "torus192": dict(kind="torus", n=(192, 192, 128), ref_cfg="torus",
                      label="Fishbone-Moncrief torus, Kerr-Schild a=0.9, MKS 192x192x128, r_in 6, r_pmax 12, "
                            "Gamma 5/3, beta 100 loop, H/R 0.1 cooling, PPM_MC+HLLE+para flux-CT, entropy fix, FP64"),
-    "torus96": dict(kind="torus", n=(96, 96, 64), ref_cfg="torus", ref_block=(24, 24, 16),
+    "torus96": dict(kind="torus", n=(96, 96, 64), ref_cfg="torus",
                     label="Fishbone-Moncrief torus as torus192 on 96x96x64 zones"),
-    "balsara1024": dict(kind="setup", setup="balsara1", n=(1024, 1, 1), ref_cfg="balsara1", ref_block=(1024, 1, 1),
+    "balsara1024": dict(kind="setup", setup="balsara1", n=(1024, 1, 1), ref_cfg="balsara1",
                         label="Balsara-1 shock tube, 1024 zones, MC + HLLE + para flux-CT, CFL 0.5, FP64"),
     "fieldloop512": dict(kind="setup", setup="field_loop", n=(512, 512, 1), ref_cfg="field_loop",
-                         ref_block=(128, 128, 1),
                          label="advected field loop 512^2, PPM_MC + HLLE + para flux-CT, FP64"),
     "linwave256": dict(kind="linwave", n=(256, 256, 256), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
-                       ref_block=(64, 64, 64),
                        label="3D periodic Minkowski linear wave 256^3, PPM_MC+HLLE+para flux-CT, FP64"),
     "linwave128": dict(kind="linwave", n=(128, 128, 128), gam=4.0 / 3.0, cour=0.4, recon=5, flux=1, bc=1, ref_cfg="linwave",
-                       ref_block=(32, 32, 32),
                        label="3D periodic Minkowski linear wave 128^3, PPM_MC+HLLE+para flux-CT, FP64"),
 }
 
@@ -256,10 +260,13 @@ def whole_job_rates(world, zones, steps, ms_max, e2e_s_max):
     return world * zones * steps / (ms_max * 1e-3), world * zones * steps / e2e_s_max
 
 
+PRECISIONS = {"fp64": 0, "fp64_fma": 2}
+
+
 def run_ours(args, wl, rank, world, device):
     import coolharm3d_b200 as hg
     n = wl["n"]
-    e, p0 = setup(wl, device)
+    e, p0 = setup(wl, device, precision=PRECISIONS[args.precision])
     # launch configuration measured on this grid's own state (restored after)
     if args.tune_steps > 0:
         tuned, tune_before, tune_after = e.autotune(steps=args.tune_steps)
@@ -318,6 +325,7 @@ def run_ours(args, wl, rank, world, device):
                vs_baseline=None, dtype="f64", data="synthetic",
                config={"workload": args.workload, "description": wl["label"], "grid": list(n),
                        "zones": zones, "parallelism": "replicas" if world > 1 else "single",
+                       "precision": args.precision,
                        "l2": "inputs larger than L2 (state arrays of %.2f GB each)" % (
                            8 * 8 * np.prod(hg.ref_shape(n)) / 1e9),
                        "e2e": "upload from pinned host memory once + K x (hg_step(1) + nfailtot readback) + download to pinned host memory once",
@@ -344,6 +352,21 @@ def run_ours(args, wl, rank, world, device):
                        "fp64_pipe_active_ncu": fp64,
                        "note": "the step is FP64-issue bound; fp64_pipe_active_ncu is the FP64 pipe's active "
                                "fraction for this kernel from the committed ncu capture"}
+    # FP64 roofline: FP64 operations per zone-update counted by ncu (fma = 2)
+    # times the measured rate, over the FP64 peak measured now on this GPU
+    ops = fp64_ops(args.workload)
+    if ops is not None:
+        peak64, _ = hg.fp64_peak(device)
+        step_tf = ops["step"] * value / world / 1e12
+        fl = ops["per_launch"].get(dom)
+        blk = {"bound": "fp64", "unit": "TFLOP/s", "peak": peak64, "peak_source": "measured now (hg_fp64_peak)",
+               "step": {"achieved": step_tf, "frac": step_tf / peak64,
+                        "fp64_ops_per_zone_update": ops["step"]}, "source": ops["source"]}
+        if fl is not None:
+            k_tf = fl * ops["scale"] / (avg_ms * 1e-3) / 1e12
+            blk["kernel"] = {"name": dom, "achieved": k_tf, "frac": k_tf / peak64,
+                             "fp64_ops_per_launch": fl * ops["scale"]}
+        out["roofline"]["fp64"] = blk
     out["e2e"] = {"value": e2e_val, "unit": "zone-updates/s",
                   "h2d_bytes_per_step": float(state_bytes) / args.steps,
                   "d2h_bytes_per_step": float(state_bytes) / args.steps + 16 + 120}
@@ -351,10 +374,29 @@ def run_ours(args, wl, rank, world, device):
     out["gpu_launches"] = int(sum(v[1] for v in kt.values()))
     if clocks:
         out["clocks"] = clocks
-    if rank == 0 and args.mixed_steps > 0:
+    if rank == 0 and args.mixed_steps > 0 and args.precision == "fp64":
         out["mixed"] = mixed_form(args, wl, device, e, p0, ms / args.steps)
+    if rank == 0 and args.fma_steps > 0 and args.precision == "fp64":
+        out["fp64_fma"] = fma_form(args, wl, device, e, p0, ms / args.steps)
     e.close()
     return out
+
+
+def fp64_ops(workload):
+    """FP64 operations (fma counted twice) per zone-update of the whole step
+    and per launch of each kernel class, from the committed ncu count
+    (profiles/fp64_ops.json); a count taken on a smaller grid of the same
+    problem is scaled to this one by its zones per launch."""
+    try:
+        rec = json.load(open(os.path.join(HERE, "profiles", "fp64_ops.json")))
+    except (OSError, ValueError):
+        return None
+    for name, r in rec.get("workloads", {}).items():
+        if workload in r.get("applies_to", [name]):
+            zones = float(np.prod(WORKLOADS[workload]["n"]))
+            return {"step": r["per_zone_update"], "per_launch": r["per_launch"],
+                    "scale": zones / float(np.prod(r["grid"])), "source": r["command"]}
+    return None
 
 
 VARS = ["rho", "u", "U1", "U2", "U3", "B1", "B2", "B3"]
@@ -405,32 +447,159 @@ def mixed_form(args, wl, device, e64, p0, fp64_ms):
     return res
 
 
-def reference_exe(cfg):
-    return os.path.join(HERE, "oracle", "_ref", cfg, "harm3d")
+def fma_form(args, wl, device, e64, p0, fp64_ms):
+    """The FP64 form with fused multiply-adds on the same workload: its device
+    time per step, and after args.fma_steps steps the per-variable relative L1
+    difference from the plain FP64 run (beside the difference a one-ulp
+    change of u in the initial state makes to the plain run itself)."""
+    ef, _ = setup(wl, device, precision=2, p_init=p0)
+    if args.tune_steps > 0:
+        ef.autotune(steps=args.tune_steps)
+    ef.step(args.warmup)
+    ef.upload(p0)
+    ef.set_time(ef.desc.t, ef.desc.dx[0])
+    ef.step(args.steps)
+    fma_ms = ef.last_step_ms() / args.steps
+    K = args.fma_steps
+    pert = p0.copy()
+    pert[..., 1] = np.nextafter(pert[..., 1], np.inf)
+    snaps = {}
+    for name, eng, start in (("fp64", e64, p0), ("fma", ef, p0), ("fp64_ulp", e64, pert)):
+        eng.upload(start)
+        eng.set_time(eng.desc.t, eng.desc.dx[0])
+        eng.step(1)
+        one = eng.download()
+        eng.step(K - 1)
+        snaps[name] = (one, eng.download(), eng.fail_counts().tolist())
+    ef.close()
+    zones = float(np.prod(wl["n"]))
+    a, b = snaps["fma"][0][3:-3, 3:-3, 3:-3], snaps["fp64"][0][3:-3, 3:-3, 3:-3]
+    scale = np.abs(b).reshape(-1, 8).max(0)
+    normwise = np.abs(a - b).reshape(-1, 8).max(0) / np.where(scale > 0, scale, 1.0)
+    return {"value": zones / (fma_ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": fma_ms,
+            "speedup_vs_fp64": fp64_ms / fma_ms, "dtype": "f64 (fused multiply-adds)",
+            "one_step_normwise_rel_vs_fp64": dict(zip(VARS, normwise.tolist())),
+            "steps_%d" % K: {"l1_rel_fma_vs_fp64": l1_rel(snaps["fma"][1], snaps["fp64"][1]),
+                             "l1_rel_fp64_one_ulp": l1_rel(snaps["fp64_ulp"][1], snaps["fp64"][1]),
+                             "nfailtot_fma": snaps["fma"][2], "nfailtot_fp64": snaps["fp64"][2]}}
 
 
-def run_reference_sample(cfg, block, steps, procs):
-    """Time the reference build: `procs` concurrent processes, each `steps`
-    steps of a `block` grid.  Returns (zone-updates/s summed, seconds)."""
-    exe = reference_exe(cfg)
-    if not os.path.exists(exe):
-        return None, "reference build %s absent (run oracle/build_ref.py where the reference sources are)" % exe
-    env = dict(os.environ, HARM_PROBE_MAXSTEPS=str(steps), HARM_PROBE_TIME="1")
+def reference_exe(cfg, native=True):
+    """The reference's own CPU build of `cfg`: built on this machine with
+    -O3 -march=native -fcommon from the staged sources (oracle/build_ref.py
+    build_native), else the portable build that travels with the repository.
+    Returns (path, how) or (None, why)."""
+    if native:
+        try:
+            sys.path.insert(0, os.path.join(HERE, "oracle"))
+            import build_ref
+            return build_ref.build_native(cfg), "gcc -O3 -march=native -fcommon (built on this host)"
+        except Exception as ex:  # the portable build still measures the reference
+            why = str(ex)
+        finally:
+            sys.path.pop(0)
+    exe = os.path.join(HERE, "oracle", "_ref", cfg, "harm3d")
+    if os.path.exists(exe):
+        return exe, "gcc -O3 -fcommon -ffp-contract=off (portable build)"
+    return None, "reference build %s absent (run oracle/build_ref.py where the reference sources are)" % exe
+
+
+def decompose(n, procs):
+    """Block decomposition of grid n over at most `procs` processes, as the
+    reference's MPI runs split it (harm_mpi.c: a x b x c ranks, each block
+    n/a x n/b x n/c): the largest process count whose factors divide n, and
+    among those the split with the least block surface.  Directions with one
+    zone are not split.  Returns (counts, block)."""
+    best = None
+    for p in range(procs, 0, -1):
+        for a in range(1, p + 1):
+            if p % a or n[0] % a:
+                continue
+            for b in range(1, p // a + 1):
+                if (p // a) % b or n[1] % b:
+                    continue
+                c = p // a // b
+                if n[2] % c:
+                    continue
+                blk = (n[0] // a, n[1] // b, n[2] // c)
+                if any(x == 1 and m > 1 for x, m in zip(blk, n)) and p > 1:
+                    continue
+                surf = sum(blk[x] * blk[y] for x, y in ((0, 1), (0, 2), (1, 2)))
+                if best is None or surf < best[0]:
+                    best = (surf, (a, b, c), blk)
+        if best is not None:
+            return best[1], best[2]
+    return (1, 1, 1), tuple(n)
+
+
+def run_reference_blocks(exe, block, procs, warmup, steps):
+    """`procs` concurrent processes of the reference build, each advancing a
+    `block` grid by warmup + steps steps; only the last `steps` are timed
+    (the probe's own clock around step_ch()).  Returns (zone-updates/s of the
+    whole ensemble, seconds of the slowest process for the timed steps) or
+    (None, why)."""
+    env = dict(os.environ, HARM_PROBE_MAXSTEPS=str(warmup + steps), HARM_PROBE_TIME="1",
+               HARM_PROBE_TIME_SKIP=str(warmup))
     tds, ps = [], []
     for _ in range(procs):
         td = tempfile.mkdtemp()
         tds.append(td)
         ps.append(subprocess.Popen([exe, "1", "1", "1"] + [str(x) for x in block], cwd=td, env=env,
                                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
-    rates = []
+    secs, cells = [], None
     for p in ps:
-        outp, _ = p.communicate(timeout=900)
+        outp, _ = p.communicate(timeout=1800)
         m = re.search(r"probe_time steps=(\d+) seconds=([0-9.eE+-]+) cells=(\d+)", outp)
-        if not m:
-            return None, "reference run produced no timing line"
-        st, sec, cells = int(m.group(1)), float(m.group(2)), int(m.group(3))
-        rates.append(st * cells / sec)
-    return float(sum(rates)), None
+        if not m or int(m.group(1)) != steps:
+            return None, "reference run produced no timing line for %d steps" % steps
+        secs.append(float(m.group(2)))
+        cells = int(m.group(3))
+    slowest = max(secs)
+    return procs * steps * cells / slowest, slowest
+
+
+def reference_arm(wl, ncores, warmup, steps, full_grid=False):
+    """The reference's CPU build on this host's cores, on the workload's own
+    grid: split into one block per core (decompose), every block advanced by
+    its own process (no halo exchange: an upper bound on the MPI build's
+    rate, MPI being absent from the image).  1D/2D grids run one whole-grid
+    replica per core instead.  full_grid adds one single-process step of the
+    whole grid (after one warm-up step)."""
+    exe, how = reference_exe(wl["ref_cfg"])
+    if exe is None:
+        return None, how
+    n = wl["n"]
+    procs = max(1, min(ncores, 64))
+    if min(n) > 1:
+        counts, block = decompose(n, procs)
+        procs = counts[0] * counts[1] * counts[2]
+        layout = "%dx%dx%d blocks of %s" % (counts + ("x".join(map(str, block)),))
+    else:
+        block, layout = tuple(n), "%d replicas of the whole grid" % procs
+    value, slowest = run_reference_blocks(exe, block, procs, warmup, steps)
+    if value is None:
+        return None, slowest
+    zones_step = procs * int(np.prod(block))
+    res = {"value": value, "ms_per_step": 1e3 * slowest / steps, "procs": procs, "block": list(block),
+           "build": how, "cpu": _cpu_model(),
+           "sample": "%s of the %s grid, one process per core, %d untimed + %d timed steps each "
+                     "(reference CPU build, no MPI halo exchange); %d zones per step" % (
+                         layout, "x".join(map(str, n)), warmup, steps, zones_step)}
+    if full_grid and min(n) > 1:
+        v1, s1 = run_reference_blocks(exe, tuple(n), 1, 1, 1)
+        if v1 is not None:
+            res["single_process_full_grid"] = {"value": v1, "ms_per_step": 1e3 * s1, "steps": 1, "warmup": 1}
+    return res, None
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def main():
@@ -443,26 +612,18 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        procs = max(1, min(ncores, 64))
-        rate, err = run_reference_sample(wl["ref_cfg"], wl["ref_block"], 1, procs)
-        if rate is None:
+        res, err = reference_arm(wl, ncores, max(1, args.warmup), args.steps, full_grid=True)
+        if res is None:
             print(json.dumps({"impl": "reference", "unavailable": err}))
             return 0
-        # the timed steps of the arm: K bounded samples
-        ks = []
-        for _ in range(max(1, min(args.steps, 2))):
-            r, _ = run_reference_sample(wl["ref_cfg"], wl["ref_block"], 1, procs)
-            ks.append(r)
-        value = float(np.median(ks))
-        zones = np.prod(wl["n"])
-        sample = "%d processes x 1 step of the %s block each (one rank's block of %s), reference CPU build, no MPI" % (
-            procs, "x".join(map(str, wl["ref_block"])), "x".join(map(str, wl["n"])))
+        value = res["value"]
         out = dict(impl="reference", metric="zone-updates/s", value=value, unit="zone-updates/s", n_gpus=world,
-                   steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * zones / value, higher_is_better=True,
-                   scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-                   config={"workload": args.workload, "description": wl["label"], "grid": list(wl["n"])},
-                   cpu_baseline={"value": value, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
-                                 "sample": sample},
+                   steps=args.steps, warmup=max(1, args.warmup), ms_per_step=res["ms_per_step"],
+                   higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                   config={"workload": args.workload, "description": wl["label"], "grid": list(wl["n"]),
+                           "reference": {k: v for k, v in res.items() if k not in ("value", "ms_per_step")}},
+                   cpu_baseline={"value": value, "unit": "zone-updates/s", "cores": res["procs"],
+                                 "kind": "reference", "sample": res["sample"]},
                    e2e={"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
         print(json.dumps(out))
         return 0
@@ -474,12 +635,12 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     out = run_ours(args, wl, rank, world, local)
     if rank == 0 and not args.no_cpu_baseline:
-        procs = max(1, min(ncores, 64))
-        rate, err = run_reference_sample(wl["ref_cfg"], wl["ref_block"], 1, procs)
-        if rate is not None:
-            out["cpu_baseline"] = {"value": rate, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
-                                   "sample": "%d processes x 1 step of a %s block (reference CPU build, no MPI)" % (
-                                       procs, "x".join(map(str, wl["ref_block"])))}
+        # a bounded sample of the same measurement: 1 untimed + 2 timed steps
+        res, err = reference_arm(wl, ncores, 1, 2)
+        if res is not None:
+            out["cpu_baseline"] = {"value": res["value"], "unit": "zone-updates/s", "cores": res["procs"],
+                                   "kind": "reference", "sample": res["sample"], "build": res["build"],
+                                   "cpu": res["cpu"], "ms_per_step": res["ms_per_step"]}
         else:
             out["cpu_baseline"] = {"value": None, "unit": "zone-updates/s", "cores": 0, "kind": "reference",
                                    "sample": err}

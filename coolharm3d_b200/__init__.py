@@ -48,7 +48,7 @@ EXPORTS = ["hg_check_mirror", "hg_init", "hg_set_geometry", "hg_set_cell_data", 
            "hg_build_geometry_ks_mks", "hg_fixup_bounds", "hg_batch_create", "hg_batch_add", "hg_batch_remove",
            "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes",
            "hg_get_totals", "hg_get_launch_config", "hg_set_launch_config", "hg_autotune",
-           "hg_write_rdump", "hg_read_rdump"]
+           "hg_write_rdump", "hg_read_rdump", "hg_fp64_peak"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 class LaunchConfig(ctypes.Structure):
@@ -105,6 +105,7 @@ def load_library(path=LIB_PATH):
     lib.hg_batch_step.argtypes = [P, P, P]
     lib.hg_batch_destroy.argtypes = [P]
     lib.hg_mem_info.argtypes = [ctypes.c_int32, P, P]
+    lib.hg_fp64_peak.argtypes = [ctypes.c_int32, P, P]
     lib.hg_get_totals.argtypes = [P, P, P, P]
     lib.hg_get_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
     lib.hg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
@@ -349,6 +350,13 @@ def mem_info(device=0):
     f, t = ctypes.c_uint64(), ctypes.c_uint64()
     _check(load_library().hg_mem_info(device, ctypes.byref(f), ctypes.byref(t)), "hg_mem_info")
     return f.value, t.value
+
+
+def fp64_peak(device=0):
+    """(TFLOP/s, ms) of the device's measured FP64 fused-multiply-add peak."""
+    tf, ms = ctypes.c_double(), ctypes.c_double()
+    _check(load_library().hg_fp64_peak(device, ctypes.byref(tf), ctypes.byref(ms)), "hg_fp64_peak")
+    return tf.value, ms.value
 
 
 def pinned_array(shape, dtype=np.float64):

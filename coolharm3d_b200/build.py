@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libharmgpu.so")
-SOURCES = ["hg_kernels.cu", "hg_api.cu", "hg_geometry.cu", "hg_mixed.cu"]
+SOURCES = ["hg_kernels.cu", "hg_api.cu", "hg_geometry.cu", "hg_mixed.cu", "hg_peak.cu"]
 # (object name, source, extra flags): the step kernels once more with fused
 # multiply-adds, into namespace hg_fma (HG_PREC_FP64_FMA)
 EXTRA_OBJECTS = [("hg_kernels_fma.o", "hg_kernels.cu", ["-fmad=true", "-DHG_FMA_BUILD"])]

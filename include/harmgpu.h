@@ -208,6 +208,13 @@ int hg_write_rdump(hg_handle *h, const char *path, int32_t nstep, const int32_t 
 int hg_read_rdump(hg_handle *h, const char *path, int32_t *nstep, int32_t n_out[HG_N_OUT_TYPES],
                   int32_t *rdump_cnt);
 
+/* The device's FP64 peak in TFLOP/s, measured: a kernel of nothing but
+ * independent FP64 fused multiply-add chains on every SM (one fma = two
+ * operations), best of five timed launches; *ms (may be NULL) gets that
+ * launch's duration.  The denominator of the step's FP64 roofline fraction.
+ * No reference counterpart. */
+int hg_fp64_peak(int32_t device, double *tflops, double *ms);
+
 /* Device time of the last hg_step call in milliseconds (CUDA events). */
 int hg_last_step_ms(hg_handle *h, double *ms);
 

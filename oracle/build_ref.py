@@ -187,6 +187,59 @@ def build(cfg, jobs=8):
     return exe
 
 
+NATIVE_FLAGS = ["-O3", "-march=native", "-fcommon", "-w"]
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def build_native(cfg, jobs=None):
+    """The reference's own build for timing on this machine: the sources staged
+    in oracle/_ref/<cfg>/src (by build()) compiled with the flags its users
+    would use, gcc -O3 -march=native -fcommon, plus the probe, into
+    oracle/_ref/<cfg>/harm3d_native; a stamp records the CPU it was built for.
+    Needs no reference checkout: the staged sources travel with oracle/_ref.
+    Returns the executable, rebuilt only when the CPU differs."""
+    bdir = os.path.join(OUT, cfg)
+    sdir = os.path.join(bdir, "src")
+    exe = os.path.join(bdir, "harm3d_native")
+    stamp = exe + ".cpu"
+    model = cpu_model()
+    if os.path.exists(exe) and os.path.exists(stamp) and open(stamp).read() == model:
+        return exe
+    if not os.path.isdir(sdir):
+        raise RuntimeError("no staged reference sources in %s (run oracle/build_ref.py where the reference is)" % sdir)
+    init_file = CONFIGS[cfg][0]
+    odir = os.path.join(bdir, "obj_native")
+    os.makedirs(odir, exist_ok=True)
+    srcs = [os.path.join(sdir, x) for x in BASE_SRCS + [init_file]] + [os.path.join(HERE, "ref_probe.c")]
+    jobs = jobs or max(1, os.cpu_count() or 1)
+    procs, objs = [], []
+    for src in srcs:
+        o = os.path.join(odir, os.path.basename(src)[:-2] + ".o")
+        extra = ["-Dstep_ch=ref_step_ch"] if os.path.basename(src) == "step_ch.c" else []
+        objs.append(o)
+        procs.append(subprocess.Popen(["gcc"] + NATIVE_FLAGS + ["-I", sdir] + extra + ["-c", src, "-o", o]))
+        if len(procs) >= jobs:
+            if procs.pop(0).wait() != 0:
+                raise RuntimeError("build_ref: native compile failed for " + cfg)
+    for p in procs:
+        if p.wait() != 0:
+            raise RuntimeError("build_ref: native compile failed for " + cfg)
+    subprocess.check_call(["gcc", "-o", exe + ".tmp"] + objs + ["-lm"])
+    os.replace(exe + ".tmp", exe)
+    with open(stamp, "w") as f:
+        f.write(model)
+    return exe
+
+
 def main(argv):
     cfgs = argv or sorted(CONFIGS)
     if not os.path.isdir(REF_SRC):

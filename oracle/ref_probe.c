@@ -14,6 +14,9 @@
  *   HARM_PROBE_MAXSTEPS=N      stop (exit 0) after N steps
  *   HARM_PROBE_TIME=1          print one line "probe_time steps=<n> seconds=<s>
  *                              cells=<NCELLS>" timing only the step calls
+ *   HARM_PROBE_TIME_SKIP=k     leave the first k steps out of that timing
+ *                              (warm-up: first-call set-up such as the
+ *                              cooling tables of phys.c:683-704)
  *   HARM_PROBE_FINAL=1         write <prefix>.<nstep>.bin after the step that
  *                              reaches t >= GridLength[0] (where main()'s loop,
  *                              main.c:64, ends the run) and exit 0
@@ -41,6 +44,7 @@ static long probe_maxsteps = -1;
 static double probe_seconds = 0.;
 static long probe_steps = 0;
 static int probe_time = 0;
+static long probe_skip = 0;
 
 static int should_dump(int n)
 {
@@ -179,8 +183,8 @@ static double now_s(void)
 static void probe_finish(void)
 {
   if (probe_time) {
-    printf("probe_time steps=%ld seconds=%.9f cells=%ld\n", probe_steps, probe_seconds,
-           (long)NCELLS);
+    printf("probe_time steps=%ld seconds=%.9f cells=%ld\n", probe_steps - (probe_skip < probe_steps ? probe_skip : probe_steps),
+           probe_seconds, (long)NCELLS);
     fflush(stdout);
   }
 }
@@ -196,11 +200,14 @@ void step_ch(void)
     const char *ms = getenv("HARM_PROBE_MAXSTEPS");
     if (ms) probe_maxsteps = atol(ms);
     probe_time = getenv("HARM_PROBE_TIME") != NULL;
+    const char *sk = getenv("HARM_PROBE_TIME_SKIP");
+    if (sk) probe_skip = atol(sk);
     if (should_dump(0)) dump_state(0);
   }
-  double t0 = probe_time ? now_s() : 0.;
+  const int timed = probe_time && probe_steps >= probe_skip;
+  double t0 = timed ? now_s() : 0.;
   ref_step_ch();
-  if (probe_time) probe_seconds += now_s() - t0;
+  if (timed) probe_seconds += now_s() - t0;
   probe_steps++;
   /* main() increments nstep after this returns; report the step count done */
   int done = nstep + 1;

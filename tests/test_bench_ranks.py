@@ -63,3 +63,13 @@ def test_reference_arm_runs_on_rank_0_only():
                         "--steps", "1", "--warmup", "3"], env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_splits_the_grid_like_an_mpi_run():
+    """The reference arm times the workload's own grid split into one block
+    per core, with the least block surface (least ghost work per zone)."""
+    assert bench.decompose((192, 192, 128), 16) == ((2, 4, 2), (96, 48, 64))
+    assert bench.decompose((192, 192, 128), 8) == ((2, 2, 2), (96, 96, 64))
+    assert bench.decompose((192, 192, 128), 64) == ((4, 4, 4), (48, 48, 32))
+    counts, block = bench.decompose((192, 192, 128), 12)
+    assert counts[0] * counts[1] * counts[2] == 12 and all(n % c == 0 for n, c in zip((192, 192, 128), counts))

@@ -1,0 +1,108 @@
+"""The FP64 form with fused multiply-adds (precision HG_PREC_FP64_FMA).
+
+The same kernels as the plain FP64 form, compiled with contracted
+multiply-adds: every FP64 operation is still IEEE double, but a*b+c is
+rounded once instead of twice, so results move by rounding, not bit for bit.
+Measured against the reference's fixtures (differences relative to the
+largest magnitude of each variable on the grid, zone by zone):
+  * one step of smooth states (Balsara-1, the torus's own initial data):
+    within 1e-11 (1e-13 but for the torus's B3, whose largest value is small),
+    pflag and every failure counter exactly equal;
+  * one step of the stress states (extreme densities, Lorentz factors and
+    magnetisations): up to ~1e-7, because their inversions are
+    ill-conditioned and amplify the last bit;
+  * Balsara-1 to t = 0.4: relative L1 ~1e-13, within the 1e-10 bar;
+  * one period of the slow wave: relative L1 up to ~3e-3 in the velocities:
+    the PPM limiter's branches (extremum and monotonicity tests) flip on
+    last-bit differences at the wave's crests, so two roundings of the same
+    scheme part by the limiter's own O(1) choices.
+So this form does not meet the drop-in's parity bar (the plain FP64 form
+matches the reference bit for bit on the same runs) and is not the default.
+"""
+import numpy as np
+import pytest
+
+import coolharm3d_b200 as hg
+import fixtures
+import harmtest as ht
+from test_t_final import WHOLE_RUNS, l1_rel
+
+pytestmark = pytest.mark.gpu
+
+ONE_STEP_TOL = 1e-11
+L1_BAR = 1e-10
+
+
+def fma_engine(f):
+    from test_gpu_parity import engine_for
+    sw = dict(f["sw"])
+    e, cell6 = engine_for(f["n"], sw, f, f["p0"], f["t0"], f["dt0"])
+    e.close()
+    d = hg.make_desc(f["n"], f["gam"], f["cour"], f["dx"], f["startx"], f["grid_length"], t=f["t0"],
+                     recon=sw["recon"], flux=sw["flux"], ct_para=sw["ct_para"], bc=sw["bc"],
+                     metric_dim=sw["metric_dim"], use_ee=sw["ee"], cooling=sw["cooling"],
+                     rescale_r=sw["rescale"], precision=hg.PREC_FP64_FMA)
+    e = hg.Engine(d)
+    if sw["metric_dim"] == 0:
+        geom, c6 = hg.minkowski_tables(d)
+        e.set_geometry(geom)
+        e.set_cell_data(c6)
+    else:
+        e.set_geometry(f["geom"], f["conn"])
+        e.set_cell_data(cell6, f["rface"] if sw["rescale"] else None)
+    if sw["cooling"]:
+        e.set_cooling_tables(f["cool_omega"], f["cool_temp"])
+    e.upload(f["p0"])
+    e.set_time(f["t0"], f["dt0"])
+    return e
+
+
+def normwise_rel(a, b):
+    """max over zones of |a - b| / max|b| per variable (physical zones)."""
+    scale = np.abs(b).reshape(-1, 8).max(0)
+    return (np.abs(a - b).reshape(-1, 8).max(0) / np.where(scale > 0, scale, 1.0))
+
+
+ONE_STEP = [n for n in fixtures.names() if n.endswith("_s1")]
+
+
+@pytest.mark.parametrize("name", ONE_STEP)
+def test_fma_one_step(name):
+    f = fixtures.load(name)
+    e = fma_engine(f)
+    e.step(f["steps"])
+    p = e.download()
+    d = normwise_rel(ht.interior(p, f["n"]), ht.interior(f["p"], f["n"]))
+    print(name, "normwise relative difference per variable", d)
+    assert np.array_equal(e.pflag(), f["pflag"])
+    assert e.fail_counts().tolist() == f["nfailtot"].tolist()
+    assert d.max() <= (1e-7 if "stress" in name else ONE_STEP_TOL)
+    e.close()
+
+
+@pytest.mark.parametrize("name,bound", [("balsara1_n1024_tfinal", L1_BAR), ("linwave_2d_32x32x1_tfinal", 1e-2)])
+def test_fma_final_time_l1(name, bound):
+    f = fixtures.load(name)
+    e = fma_engine(f)
+    t, _ = e.step(f["steps"])
+    d = l1_rel(e.download(), f["p"], f["n"])
+    print(name, "L1 per variable", d)
+    assert (d <= bound).all()
+    assert e.fail_counts().tolist() == f["nfailtot"].tolist()
+    e.close()
+
+
+@pytest.mark.parametrize("name", [n for n in fixtures.names() if n not in ONE_STEP and n not in WHOLE_RUNS
+                                  and n not in fixtures.CHAOTIC])
+def test_fma_multi_step_fixtures(name):
+    """Several steps: flags and counters exact, primitives within 1e-10
+    (smooth runs) or 1e-7 (stress states)."""
+    f = fixtures.load(name)
+    e = fma_engine(f)
+    e.step(f["steps"])
+    d = normwise_rel(ht.interior(e.download(), f["n"]), ht.interior(f["p"], f["n"]))
+    print(name, "normwise relative difference per variable", d)
+    assert np.array_equal(e.pflag(), f["pflag"])
+    assert e.fail_counts().tolist() == f["nfailtot"].tolist()
+    assert d.max() <= (1e-7 if "stress" in name else L1_BAR)
+    e.close()
