@@ -414,7 +414,8 @@ def mixed_form(args, wl, device, e64, p0, fp64_ms):
     step, and after args.mixed_steps steps (and at a tenth of that) the
     per-variable relative L1 difference from the FP64 run, beside the
     difference a one-ulp change of u in the initial state makes to the FP64
-    run itself (how far the flow amplifies rounding)."""
+    run itself (how far the flow amplifies rounding) and the difference the
+    FP64 run shows when its initial state is rounded once to FP32."""
     em, _ = setup(wl, device, precision=1, p_init=p0)
     if args.tune_steps > 0:
         em.autotune(steps=args.tune_steps)
@@ -427,8 +428,11 @@ def mixed_form(args, wl, device, e64, p0, fp64_ms):
     k1 = max(1, K // 10)
     pert = p0.copy()
     pert[..., 1] = np.nextafter(pert[..., 1], np.inf)
+    # the state rounded once to FP32: what a single FP32 rounding of every
+    # primitive (the floor of any form that reads FP32 states) grows into
+    r32 = p0.astype(np.float32).astype(np.float64)
     snaps = {}
-    for name, eng, start in (("fp64", e64, p0), ("mixed", em, p0), ("fp64_ulp", e64, pert)):
+    for name, eng, start in (("fp64", e64, p0), ("mixed", em, p0), ("fp64_ulp", e64, pert), ("fp64_r32", e64, r32)):
         eng.upload(start)
         eng.set_time(eng.desc.t, eng.desc.dx[0])
         eng.step(k1)
@@ -443,7 +447,8 @@ def mixed_form(args, wl, device, e64, p0, fp64_ms):
     for idx, steps in ((0, k1), (1, K)):
         res["accuracy"]["steps_%d" % steps] = {
             "l1_rel_mixed_vs_fp64": l1_rel(snaps["mixed"][idx], snaps["fp64"][idx]),
-            "l1_rel_fp64_one_ulp": l1_rel(snaps["fp64_ulp"][idx], snaps["fp64"][idx])}
+            "l1_rel_fp64_one_ulp": l1_rel(snaps["fp64_ulp"][idx], snaps["fp64"][idx]),
+            "l1_rel_fp64_from_fp32_rounded_state": l1_rel(snaps["fp64_r32"][idx], snaps["fp64"][idx])}
     return res
 
 

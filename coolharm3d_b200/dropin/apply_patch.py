@@ -4,11 +4,15 @@
   python apply_patch.py <src-dir>
 
 Adds hg_driver.c (the driver's side of libharmgpu, beside this script) to
-<src-dir> and inserts, each inside `#if USE_GPU_STEP`, four calls:
+<src-dir> and inserts, each inside `#if USE_GPU_STEP`, five calls:
   step_ch.c  first statement of step_ch():      if (hg_gpu_step()) return;
   main.c     after global_init():               hg_gpu_init();
              after the loop's nstep++:          hg_gpu_sync_host(0);
              before the final restart_write():  hg_gpu_sync_host(1);
+  diag.c     dump_ener(), after its flux totals
+             are scaled:                         hg_gpu_totals(U_tot, F_tot);
+(dump_ener integrates the last substep's conserved variables and boundary
+fluxes, which stay on the device: the library sums them there.)
 Built without -DUSE_GPU_STEP=1 the sources compile to the unchanged CPU
 program.  Build with -DUSE_GPU_STEP=1 -I<repo>/include, add hg_driver.c to
 the sources, and link -L<repo>/coolharm3d_b200 -lharmgpu
@@ -44,8 +48,9 @@ def hook(indent, call):
 def apply(src):
     sc = os.path.join(src, "step_ch.c")
     mc = os.path.join(src, "main.c")
-    s, m = open(sc).read(), open(mc).read()
-    if MARK in s or MARK in m:
+    dc = os.path.join(src, "diag.c")
+    s, m, dg = open(sc).read(), open(mc).read(), open(dc).read()
+    if MARK in s or MARK in m or MARK in dg:
         raise RuntimeError("already patched: " + src)
     # the first statement of step_ch(): after the line holding its opening brace
     i = s.index("void step_ch(void)")
@@ -56,8 +61,11 @@ def apply(src):
     m = _insert(m, r"^\s*nstep\+\+\s*;", hook("\t\t", "{ extern void hg_gpu_sync_host(int); hg_gpu_sync_host(0); }"))
     m = _insert(m, r"^\s*restart_write\(\)\s*;", hook("\t", "{ extern void hg_gpu_sync_host(int); hg_gpu_sync_host(1); }"),
                 before=True, last=True)
+    dg = _insert(dg, r"^\s*PLOOP\s+F_tot\[2\]\[BCUP\]\[l\]\s*\*=",
+                 hook("  ", "{ extern void hg_gpu_totals(double *, double *); hg_gpu_totals(U_tot, &F_tot[0][0][0]); }"))
     open(sc, "w").write(s)
     open(mc, "w").write(m)
+    open(dc, "w").write(dg)
     shutil.copy(os.path.join(HERE, "hg_driver.c"), os.path.join(src, "hg_driver.c"))
 
 

@@ -1,6 +1,6 @@
 /* hg_driver.c -- the HARM3D driver's side of libharmgpu: compiled into the
  * reference's own build (next to main.c and step_ch.c, with its decs.h) when
- * USE_GPU_STEP is 1.  Three hooks connect it (INTEGRATION.md shows the
+ * USE_GPU_STEP is 1.  Five hooks connect it (INTEGRATION.md shows the
  * patch, tests/test_dropin.py applies it and compares the result):
  *
  *   main.c, after global_init():     hg_gpu_init();        the grid goes to the GPU
@@ -8,6 +8,10 @@
  *   main.c, after nstep++ and after
  *   the time loop:                   hg_gpu_sync_host(0 / 1);  p comes back when
  *                                    diag() or restart_write() will read it
+ *   diag.c, dump_ener(), after the
+ *   flux totals are scaled:          hg_gpu_totals(U_tot, F_tot);  the integrals
+ *                                    of the last substep's U and boundary fluxes,
+ *                                    summed on the device
  *
  * Everything else of the driver (init.*.c, diag(), restart_write(),
  * check_for_crash()) is unchanged and reads the globals this file keeps
@@ -163,5 +167,23 @@ void hg_gpu_sync_host(int force)
   }
   free(pf);
   free(pg);
+}
+
+/* dump_ener()'s integrals (diag.c:745-766) from the device: dV times the sum
+ * of the last substep's conserved variables over the physical zones, and the
+ * face area times the sum of its fluxes over each physical boundary plane
+ * (0 where the boundary is not physical, as dump_ener leaves it).  Sums are
+ * per block and then in block order: within rounding of dump_ener's
+ * sequential sums. */
+void hg_gpu_totals(double *U_tot, double *F_tot)
+{
+  int d, side, l;
+  double u[8], f[48];
+  hg_check(hg_get_totals(gpu_grid, u, f, NULL), "hg_get_totals");
+  for (l = 0; l < NP; l++) U_tot[l] = u[l];
+  for (d = 0; d < NDIM - 1; d++)
+    for (side = 0; side < 2; side++)
+      for (l = 0; l < NP; l++)
+        F_tot[(d * 2 + side) * NP + l] = (bc_pid[d + 1][side] == BC_PHYS) ? f[(d * 2 + side) * 8 + l] : 0.;
 }
 #endif /* USE_GPU_STEP */

@@ -232,6 +232,78 @@ def summarize(results):
             "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "steps": int(sum(r.steps for r in results))}
 
 
+def _class_key(req):
+    return (req.kind, req.size, req.precision)
+
+
+def measure_classes(stream, device=0, steps=20, copies=8):
+    """Per request class (kind, size, precision) of the stream: the CFL
+    time step (the setups start from dx[0] = 1e-5, which timestep() grows
+    by at most 1.3x per step; stepped until it stops growing, at most 120
+    steps), and the zone-update rate of one grid stepped alone (hg_step)
+    and of `copies` grids stepped together in one batch (the most the
+    device gives that class), each over `steps` steps."""
+    out = {}
+    for key in sorted({_class_key(r) for r in stream}):
+        req = Request(-1, key[0], key[1], key[2], 0.0)
+        prob = req.problem(device)
+        engs = []
+        try:
+            for _ in range(copies):
+                e = Engine(prob.desc)
+                setups.start(e, prob)
+                engs.append(e)
+            dt = 0.0
+            for _ in range(120):
+                t, dt_new = engs[0].step(1)
+                if dt_new <= dt * 1.0001:
+                    dt = dt_new
+                    break
+                dt = dt_new
+            engs[0].step(steps)
+            alone = prob.zones * steps / (engs[0].last_step_ms() * 1e-3)
+            b = Batch(device, copies)
+            for e in engs:
+                b.add(e)
+            b.step()
+            b.step()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                b.step()
+            batched = copies * prob.zones * steps / (time.perf_counter() - t0)
+            for e in engs:
+                b.remove(e)
+            b.close()
+        finally:
+            for e in engs:
+                e.close()
+        out[key] = {"dt": dt, "zones": prob.zones, "t_final": prob.t_final, "alone": alone, "batched": batched}
+    return out
+
+
+def stream_bound(stream, classes):
+    """How much batching can gain on this stream at most.  Request r needs
+    W_r = zones x steps zone-updates (steps = t_final / dt of its class).
+    Sequentially it takes W_r / alone_rate; perfectly packed into batches it
+    takes at least W_r / batched_rate (its class at full occupancy), so the
+    speedup of any batching of the stream is at most
+    sum(W_r / alone) / sum(W_r / batched).  Also returns each kind's share of
+    the zone-updates and of the sequential time."""
+    seq, best = 0.0, 0.0
+    share_w, share_t = {}, {}
+    for r in stream:
+        c = classes[_class_key(r)]
+        w = c["zones"] * np.ceil(c["t_final"] * r.time_scale / c["dt"])
+        seq += w / c["alone"]
+        best += w / c["batched"]
+        share_w[r.kind] = share_w.get(r.kind, 0.0) + w
+        share_t[r.kind] = share_t.get(r.kind, 0.0) + w / c["alone"]
+    tw, tt = sum(share_w.values()), sum(share_t.values())
+    return {"max_speedup": seq / best, "sequential_s": seq, "best_batched_s": best,
+            "zone_update_share": {k: v / tw for k, v in share_w.items()},
+            "sequential_time_share": {k: v / tt for k, v in share_t.items()}}
+
+
 def main(argv=None):
     import argparse
     import json
@@ -241,10 +313,19 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--time-scale", type=float, default=1.0)
     ap.add_argument("--slots", type=int, default=64)
-    ap.add_argument("--mode", choices=["batched", "sequential", "both"], default="both")
+    ap.add_argument("--mode", choices=["batched", "sequential", "both", "bound"], default="both",
+                    help="bound: measure every request class alone and batched, and print the largest speedup "
+                         "batching can reach on this stream")
     a = ap.parse_args(argv)
     stream = make_stream(a.requests, a.rate, a.seed, a.time_scale)
     out = {"stream": {"requests": a.requests, "rate_per_s": a.rate, "seed": a.seed, "time_scale": a.time_scale}}
+    if a.mode == "bound":
+        cls = measure_classes(stream)
+        out["classes"] = {"%s/%d/%s" % (k[0], k[1], "mixed" if k[2] == PREC_MIXED else "fp64"): v
+                          for k, v in cls.items()}
+        out["bound"] = stream_bound(stream, cls)
+        print(json.dumps(out))
+        return 0
     runs = {}
     if a.mode in ("batched", "both"):
         runs["batched"] = serve_batched(stream, max_slots=a.slots)
