@@ -48,8 +48,40 @@ EXPORTS = ["hg_check_mirror", "hg_init", "hg_set_geometry", "hg_set_cell_data", 
            "hg_build_geometry_ks_mks", "hg_fixup_bounds", "hg_batch_create", "hg_batch_add", "hg_batch_remove",
            "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes",
            "hg_get_totals", "hg_get_launch_config", "hg_set_launch_config", "hg_autotune",
-           "hg_write_rdump", "hg_read_rdump", "hg_fp64_peak"]
+           "hg_write_rdump", "hg_read_rdump", "hg_fp64_peak", "hg_set_dynamic_metric", "hg_dyn_geometry"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
+
+DYN_MINK_SPHERICAL = 2
+
+
+class DynMetric(ctypes.Structure):
+    """hg_dyn_metric: the spacetime and COORD_DIAGONAL3 parameters of a
+    metric_dim 3 (time-dependent metric) grid."""
+    _fields_ = [("spacetime", ctypes.c_int32), ("diag3_exponent", ctypes.c_int32), ("R0", ctypes.c_double),
+                ("h_slope", ctypes.c_double), ("diag3_factor", ctypes.c_double), ("dt_conn", ctypes.c_double)]
+
+
+def dyn_metric(spacetime=DYN_MINK_SPHERICAL, R0=0.0, h_slope=0.35, th_cutout=None, diag3_exponent=7, dt_conn=9.0e-6):
+    """The torus setup's coordinates (set_special_coord, init.torus.c:245-270:
+    th_cutout = SMALL pi, diag3_factor = 1 - 2 th_cutout/pi - h_slope) and the
+    driver's dt_conn (main.c:569)."""
+    import math
+    if th_cutout is None:
+        th_cutout = 1e-15 * math.pi
+    m = DynMetric()
+    m.spacetime, m.diag3_exponent, m.R0, m.h_slope = spacetime, diag3_exponent, R0, h_slope
+    m.diag3_factor = 1. - 2 * th_cutout / math.pi - h_slope
+    m.dt_conn = dt_conn
+    return m
+
+
+def dyn_geometry(desc, m, pos, i, j, k, t=0.0):
+    """hg_dyn_geometry: the 42-double struct of_geom the device evaluates, on the host."""
+    out = np.zeros(NGEOM)
+    _check(load_library().hg_dyn_geometry(ctypes.byref(desc), ctypes.byref(m), pos, i, j, k, t, _ptr(out)),
+           "hg_dyn_geometry")
+    return out
+
 
 class LaunchConfig(ctypes.Structure):
     """hg_launch_config: blocks per launch of each kernel class and the
@@ -106,6 +138,9 @@ def load_library(path=LIB_PATH):
     lib.hg_batch_destroy.argtypes = [P]
     lib.hg_mem_info.argtypes = [ctypes.c_int32, P, P]
     lib.hg_fp64_peak.argtypes = [ctypes.c_int32, P, P]
+    lib.hg_set_dynamic_metric.argtypes = [P, P]
+    lib.hg_dyn_geometry.argtypes = [ctypes.POINTER(GridDesc), P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.c_int32, ctypes.c_double, P]
     lib.hg_get_totals.argtypes = [P, P, P, P]
     lib.hg_get_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
     lib.hg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
@@ -211,6 +246,10 @@ class Engine:
         conn = None if conn is None else np.ascontiguousarray(conn, np.float64)
         nc = 0 if conn is None else conn.size // 64
         _check(self.lib.hg_set_geometry(self.h, _ptr(geom), ng, _ptr(conn), nc), "hg_set_geometry")
+
+    def set_dynamic_metric(self, m):
+        """metric_dim 3: the time-dependent metric the device evaluates."""
+        _check(self.lib.hg_set_dynamic_metric(self.h, ctypes.byref(m)), "hg_set_dynamic_metric")
 
     def set_cell_data(self, cell6, rface=None):
         cell6 = np.ascontiguousarray(cell6, np.float64)

@@ -20,6 +20,7 @@
 
 #include "harmgpu.h"
 #include "hg_internal.h"
+#include "hg_dyn.cuh"
 
 namespace hg {
 void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec *R);
@@ -30,6 +31,7 @@ void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int 
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 cudaError_t prepare_kernels();
+void launch_geom_levels(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_totals(const GridDev &G, const LaunchCfg &L, cudaStream_t s, double *part, double *out);
 void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
                           double *out);
@@ -41,6 +43,7 @@ void launch_planes_to_ref(const GridDev &G, const LaunchCfg &L, cudaStream_t s, 
 // (hg_kernels.cu compiled with HG_FMA_BUILD): HG_PREC_FP64_FMA.
 namespace hg_fma {
 void launch_step(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s, hg::EventRec *R);
+void launch_geom_levels(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s);
 void launch_face_flux(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s, int d);
 cudaError_t prepare_kernels();
 }  // namespace hg_fma
@@ -75,6 +78,7 @@ struct hg_handle {
   bool exec_stale = true;
   bool graph_dirty = true;           // the capture predates a change of the kernels' arguments
   uint64_t capture_gen = 0;          // number of captures of step_graph so far (batches compare it)
+  bool levels_stale = false;         // metric_dim 3: the time levels predate t, dx[0] or the metric
   double *d_tot = nullptr;           // hg_get_totals: per-block partials and the result
   int batch_refs = 0;                // batches this grid belongs to
   long ntot_ref = 0;          // N1TOT*N2TOT*N3TOT of the reference layout
@@ -153,7 +157,10 @@ static int validate(const hg_grid_desc *d)
   if (d->bc_type != 0 && d->bc_type != 1 && d->bc_type != 10) return HG_ERR_BADARG;
   // the spherical boundaries need the radial and polar directions resolved
   if (d->bc_type == 10 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
-  if (d->metric_dim != 0 && d->metric_dim != 2) return HG_ERR_BADARG;
+  if (d->metric_dim != 0 && d->metric_dim != 2 && d->metric_dim != 3) return HG_ERR_BADARG;
+  // metric_dim 3 (time-dependent metric): every direction resolved, FP64 forms
+  if (d->metric_dim == 3 && (d->n1 == 1 || d->n2 == 1 || d->n3 == 1 || d->precision == HG_PREC_MIXED))
+    return HG_ERR_BADARG;
   if (d->cooling != 0 && d->cooling != 1) return HG_ERR_BADARG;
   if (d->precision != HG_PREC_FP64 && d->precision != HG_PREC_MIXED && d->precision != HG_PREC_FP64_FMA)
     return HG_ERR_BADARG;
@@ -245,6 +252,11 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
       ALLOC(G.geomT, sizeof(double) * 42 * G.gS);
       ALLOC(G.conn, sizeof(double) * 64 * G.T[0] * G.T[1]);
     }
+    if (G.mdim == 3) {  // three time levels of 42 planes of 5 positions, the substep's connection
+      G.gS3 = (long)HG_NPOS * G.S;
+      for (int l = 0; l < 3; l++) ALLOC(G.geomL[l], sizeof(double) * 42 * G.gS3);
+      ALLOC(G.conn3, sizeof(double) * 64 * G.S);
+    }
     if (G.rescale) ALLOC(G.rsc, sizeof(double) * 12 * G.T[0]);
     if (G.prec == HG_PREC_MIXED) {
       ALLOC(G.p32, sizeof(float) * HG_NPR * G.S);
@@ -292,6 +304,9 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     memset(&sc0, 0, sizeof(sc0));
     sc0.t = desc->t;
     sc0.dt = desc->dx[0];
+    sc0.lev[0] = 0;  // n_beg, n_mid, n_end (init_general_metric, metric.c:3676-3679)
+    sc0.lev[1] = 1;
+    sc0.lev[2] = 2;
     if (copy_sync(h, G.sc, &sc0, sizeof(sc0), cudaMemcpyHostToDevice) != cudaSuccess) {
       rc = HG_ERR_CUDA;
       goto fail;
@@ -330,6 +345,7 @@ extern "C" void hg_destroy(hg_handle *h)
 extern "C" int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom, const double *conn, int64_t n_conn)
 {
   if (!h || !geom) return HG_ERR_BADARG;
+  if (h->G.mdim == 3) return HG_ERR_BADARG;  // its geometry comes from hg_set_dynamic_metric
   h->graph_dirty = true;
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
@@ -679,6 +695,19 @@ extern "C" int hg_set_time(hg_handle *h, double t, double dt)
   HG_CK(cudaSetDevice(h->d.device));
   double v[2] = {t, dt};
   HG_CK(copy_sync(h, sc_field(h->G, offsetof(hg::DevScalars, t)), v, sizeof(v), cudaMemcpyHostToDevice));
+  if (h->G.mdim == 3) h->levels_stale = true;
+  return HG_OK;
+}
+
+// metric_dim 3: (re)fill the three time levels at the device's t and dx[0]
+// after the metric, t or dx[0] changed (init_general_metric, metric.c:3664)
+static int refresh_levels(hg_handle *h)
+{
+  if (h->G.mdim != 3 || !h->levels_stale) return HG_OK;
+  if (h->G.prec == HG_PREC_FP64_FMA) hg_fma::launch_geom_levels(h->G, h->L, h->stream);
+  else hg::launch_geom_levels(h->G, h->L, h->stream);
+  HG_CK(cudaGetLastError());
+  h->levels_stale = false;
   return HG_OK;
 }
 
@@ -727,6 +756,10 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
     int rc = step_exec_ready(h);
     if (rc != HG_OK) return rc;
   }
+  {
+    int rc = refresh_levels(h);
+    if (rc != HG_OK) return rc;
+  }
   HG_CK(cudaEventRecord(h->ev0, h->stream));
   for (int s = 0; s < nsteps; s++) {
     if (R) launch_grid_step(h->G, h->L, h->stream, R);
@@ -755,11 +788,63 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
   return HG_OK;
 }
 
+static int dyn_from_abi(const hg_dyn_metric *m, hg::DynMetric &dm)
+{
+  if (!m || m->spacetime != HG_DYN_MINK_SPHERICAL || m->diag3_exponent < 3 || !(m->dt_conn > 0.)) return HG_ERR_BADARG;
+  dm.spacetime = m->spacetime;
+  dm.diag3_exponent = m->diag3_exponent;
+  dm.R0 = m->R0;
+  dm.h_slope = m->h_slope;
+  dm.diag3_factor = m->diag3_factor;
+  dm.dt_conn = m->dt_conn;
+  return HG_OK;
+}
+
+extern "C" int hg_set_dynamic_metric(hg_handle *h, const hg_dyn_metric *m)
+{
+  if (!h || h->G.mdim != 3) return HG_ERR_BADARG;
+  int rc = dyn_from_abi(m, h->G.dyn);
+  if (rc != HG_OK) return rc;
+  HG_CK(cudaSetDevice(h->d.device));
+  const int lev[3] = {0, 1, 2};  // n_beg, n_mid, n_end (init_general_metric, metric.c:3676-3679)
+  HG_CK(copy_sync(h, sc_field(h->G, offsetof(hg::DevScalars, lev)), lev, sizeof(lev), cudaMemcpyHostToDevice));
+  h->levels_stale = true;
+  h->graph_dirty = true;  // the metric's parameters are kernel arguments
+  h->have_geom = true;
+  return HG_OK;
+}
+
+extern "C" int hg_dyn_geometry(const hg_grid_desc *d, const hg_dyn_metric *m, int32_t pos, int32_t i, int32_t j,
+                               int32_t k, double t, double geom[HG_NGEOM])
+{
+  if (!d || !geom || pos < 0 || pos > 4) return HG_ERR_BADARG;
+  GridDev G;
+  memset(&G, 0, sizeof(G));
+  int rc = dyn_from_abi(m, G.dyn);
+  if (rc != HG_OK) return rc;
+  for (int a = 0; a < 4; a++) {
+    G.startx[a] = d->startx[a];
+    G.dx[a] = d->dx[a];
+  }
+  hg::Geom g;
+  hg::dyn_geom(G, pos, i, j, k, t, g);
+  memcpy(geom, g.gcon, 16 * 8);
+  memcpy(geom + 16, g.gcov, 16 * 8);
+  geom[32] = g.g;
+  geom[33] = g.g_inv;
+  geom[34] = g.alpha;
+  for (int a = 0; a < 3; a++) geom[35 + a] = g.beta[a];
+  for (int a = 0; a < 4; a++) geom[38 + a] = g.ncon[a];
+  return HG_OK;
+}
+
 extern "C" int hg_fixup_bounds(hg_handle *h)
 {
   if (!h) return HG_ERR_BADARG;
   if (!h->have_geom || !h->have_cells || !h->have_prims) return HG_ERR_STATE;
   HG_CK(cudaSetDevice(h->d.device));
+  int rc = refresh_levels(h);
+  if (rc != HG_OK) return rc;
   hg::launch_fixup_bounds(h->G, h->L, h->stream);
   HG_CK(cudaGetLastError());
   HG_CK(cudaStreamSynchronize(h->stream));
@@ -773,6 +858,10 @@ extern "C" int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max
   GridDev &G = h->G;
   HG_CK(cudaSetDevice(h->d.device));
   HG_CK(cudaMemsetAsync(G.F[dir], 0, sizeof(double) * HG_NPR * G.S, h->stream));
+  {
+    int rc = refresh_levels(h);
+    if (rc != HG_OK) return rc;
+  }
   if (G.prec == HG_PREC_FP64_FMA) hg_fma::launch_face_flux(G, h->L, h->stream, dir);
   else hg::launch_face_flux(G, h->L, h->stream, dir);
   HG_CK(cudaGetLastError());
@@ -1086,6 +1175,10 @@ extern "C" int hg_batch_step(hg_batch *b, double *t, double *dt)
   }
   const int n = (int)b->members.size();
   if (n == 0) return HG_OK;
+  for (hg_handle *m : b->members) {  // metric_dim 3 members whose time levels are not yet filled
+    int rc = refresh_levels(m);
+    if (rc != HG_OK) return rc;
+  }
   // work the members queued on their own streams (uploads, set_time) comes first
   for (hg_handle *m : b->members) HG_CK(cudaStreamSynchronize(m->stream));
   HG_CK(cudaGraphLaunch(b->exec, b->stream));
@@ -1167,6 +1260,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   b += sizeof(hg::DevScalars) + 8ull * cap * (2 + HG_NPR);  // scalars, queue, flagged list
   if (d->use_entropy_eq) b += 8ull * 6 * cap;                 // entropy face fluxes of the queue
   if (d->metric_dim == 2) b += 8ull * 42 * gS + 8ull * 64 * T[0] * T[1];
+  if (d->metric_dim == 3) b += 3ull * 8 * 42 * HG_NPOS * S + 8ull * 64 * S;
   if (d->rescale_r) b += 8ull * 12 * T[0];
   if (d->cooling) b += 8ull * 2 * T[0];
   if (d->precision == HG_PREC_MIXED) {
@@ -1192,6 +1286,10 @@ extern "C" int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], do
     h->d_tot = (double *)q;
   }
   double *out = h->d_tot + 57L * 2048;
+  {
+    int rc = refresh_levels(h);
+    if (rc != HG_OK) return rc;
+  }
   hg::launch_totals(h->G, h->L, h->stream, h->d_tot, out);
   HG_CK(cudaGetLastError());
   double v[57];
@@ -1269,6 +1367,7 @@ static int snap(hg_handle *h, Snapshot &s, bool save)
   HG_CK(cp(s.nfail, G.nfail, sizeof(unsigned int) * G.S * HG_NF));
   HG_CK(cp(s.sc, G.sc, sizeof(hg::DevScalars)));
   if (!save && G.p32) hg::launch_to_f32(G, h->L.grid_upd, h->stream, G.p);  // the FP32 copy of the restored state
+  if (!save && G.mdim == 3) h->levels_stale = true;  // the time levels moved on with the candidates' steps
   HG_CK(cudaGetLastError());
   HG_CK(cudaStreamSynchronize(h->stream));
   return HG_OK;

@@ -43,6 +43,15 @@ struct Geom {
   __host__ __device__ double det() const { return g; }
 };
 
+// metric_dim 3 (the time-dependent metric path): the spacetime and the
+// COORD_DIAGONAL3 coordinate parameters its geometry is evaluated from.
+struct DynMetric {
+  int spacetime;       // HG_DYN_* of harmgpu.h
+  int diag3_exponent;
+  double R0, h_slope, diag3_factor;
+  double dt_conn;      // half-width of the connection's time difference (main.c:569)
+};
+
 // Device-resident scalars of one grid (t, dx[0], reductions, failure flags).
 struct DevScalars {
   double t, dt;
@@ -56,6 +65,7 @@ struct DevScalars {
   int err;                          // internal error status (queue overflow ...)
   double m_tot;
   double last_maxs[4];              // max_char_speed of the last corrector, as doubles
+  int lev[3];                       // metric_dim 3: geomL buffers of n_beg, n_mid, n_end
 };
 
 // Everything a kernel needs, passed by value.
@@ -97,6 +107,13 @@ struct GridDev {
   long capacity;             // N0*N1*N2
   double *blk;               // per-block partial sums of M_tot
   Geom g0;                   // metric_dim 0 geometry
+  // metric_dim 3: three time levels of geometry, each 42 planes of gS3 =
+  // 5*S doubles (index pos*S + zone offset), filled by k_geom_level; the
+  // connection of the current substep, 64 planes of S (k_conn_dyn)
+  double *geomL[3];
+  long gS3;
+  double *conn3;
+  DynMetric dyn;
 };
 
 // Fixed grid sizes of the step's kernels (grid-stride loops).

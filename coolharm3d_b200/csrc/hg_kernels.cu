@@ -26,6 +26,7 @@
 
 #include "harmgpu.h"
 #include "hg_common.cuh"
+#include "hg_dyn.cuh"
 #include "hg_fallback.cuh"
 
 // This file is compiled twice.  Plain: into namespace hg with no multiply-add
@@ -209,7 +210,8 @@ __device__ __forceinline__ double face_flux(const GridDev &G, const double *pl, 
 // k_flux: F[d] on faces [lo, lo+n) (reference indices), one thread per face.
 template <bool RS, int MDIM, int d>
 __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux(const __grid_constant__ GridDev G, const double *__restrict__ ph,
-                                                 int lo0, int lo1, int lo2, int n0, int n1, int n2, unsigned int mult)
+                                                 int lo0, int lo1, int lo2, int n0, int n1, int n2, unsigned int mult,
+                                                 int slot)
 {
   const unsigned total = (unsigned)n0 * n1 * n2;  // < 2^31 (hg_init)
   double vmax = 0.;
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux(const __grid_cons
       ctop = face_flux(G, pl, pr, G.g0, d, i, j, k, mult, G.F[d], o);
     } else {
       Geom g;
-      load_geom(G, d, i, j, g);
+      load_geom(G, d, i, j, g, k, slot);
       ctop = face_flux(G, pl, pr, g, d, i, j, k, mult, G.F[d], o);
     }
     if (d == 0 && G.bc == 10) {  // fix_flux(), bounds.c:2263-2275: no mass inflow through r_in, r_out
@@ -436,8 +438,8 @@ __global__ void __launch_bounds__(HG_BLK) k_emf(GridDev G, int lo0, int lo1, int
 // gamma_calc): the predictor's sources are evaluated at p_i, whose state the
 // conserved variables already needed.
 template <bool PRE>
-__device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, const Geom &g, int i, int j, double *dU,
-                                            const State &qpre, int badpre)
+__device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, const Geom &g, int i, int j, int k,
+                                            double *dU, const State &qpre, int badpre)
 {
 #pragma unroll
   for (int l = 0; l < HG_NPR; l++) dU[l] = 0.;
@@ -451,15 +453,28 @@ __device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, 
     mhd_row(q, 1, mhd[1]);
     mhd_row(q, 2, mhd[2]);
     mhd_row(q, 3, mhd[3]);
-    const long cS = (long)G.T[0] * G.T[1];
-    const long co = (long)(G.deg[1] ? 0 : j) * G.T[0] + (G.deg[0] ? 0 : i);
+    if (G.mdim == 3) {  // METRIC_DIM > 2: all four components (phys.c:143-154)
+      const long cS = G.S, co = off3(G, i, j, k);
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+      for (int a = 0; a < 4; a++)
 #pragma unroll
-      for (int b = 0; b < 4; b++) {
-        dU[U1] += mhd[a][b] * __ldg(G.conn + ((b * 4 + 1) * 4 + a) * cS + co);
-        dU[U2] += mhd[a][b] * __ldg(G.conn + ((b * 4 + 2) * 4 + a) * cS + co);
-      }
+        for (int b = 0; b < 4; b++) {
+          dU[U1] += mhd[a][b] * G.conn3[((b * 4 + 1) * 4 + a) * cS + co];
+          dU[U2] += mhd[a][b] * G.conn3[((b * 4 + 2) * 4 + a) * cS + co];
+          dU[UU] += mhd[a][b] * G.conn3[((b * 4 + 0) * 4 + a) * cS + co];
+          dU[U3] += mhd[a][b] * G.conn3[((b * 4 + 3) * 4 + a) * cS + co];
+        }
+    } else {
+      const long cS = (long)G.T[0] * G.T[1];
+      const long co = (long)(G.deg[1] ? 0 : j) * G.T[0] + (G.deg[0] ? 0 : i);
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          dU[U1] += mhd[a][b] * __ldg(G.conn + ((b * 4 + 1) * 4 + a) * cS + co);
+          dU[U2] += mhd[a][b] * __ldg(G.conn + ((b * 4 + 2) * 4 + a) * cS + co);
+        }
+    }
   }
   if (G.cooling == 1) {  // phys.c:162-172, source_cooling_func phys.c:541-582
     if (G.mdim == 0) bad = PRE ? badpre : get_state(ph, g, G.gam, q);
@@ -548,7 +563,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __gr
     const int k = HG_NGH + (int)(tq / N1);
     const long o = off3(G, i, j, k);
     Geom gl;
-    if (MDIM != 0) load_geom(G, 3, i, j, gl);
+    if (MDIM != 0) load_geom(G, 3, i, j, gl, k, 0);
     const Geom &g = (MDIM == 0) ? G.g0 : gl;
     double pi[HG_NPR], U[HG_NPR], dU[HG_NPR];
 #pragma unroll
@@ -561,7 +576,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __gr
     if (bad_i && sub == 0) book(G, NF_GAMMA_CALC, i, j, k);
     primtoflux(pi, q, 0, g, U);
     if (sub == 0) {
-      if (source_terms<true>(G, pi, g, i, j, dU, q, bad_i)) book(G, NF_GAMMA_CALC, i, j, k);
+      if (source_terms<true>(G, pi, g, i, j, k, dU, q, bad_i)) book(G, NF_GAMMA_CALC, i, j, k);
     } else {
       double phv[HG_NPR];
 #pragma unroll
@@ -569,7 +584,13 @@ __global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __gr
         const double v = p_h[l * S + o];
         phv[l] = RS ? rs_roundtrip(G, v, l, i) : v;
       }
-      if (source_terms<false>(G, phv, g, i, j, dU, q, 0)) book(G, NF_GAMMA_CALC, i, j, k);
+      if (MDIM == 3) {  // the corrector's sources take the geometry of n_mid
+        Geom gh;
+        load_geom(G, 3, i, j, gh, k, 1);
+        if (source_terms<false>(G, phv, gh, i, j, k, dU, q, 0)) book(G, NF_GAMMA_CALC, i, j, k);
+      } else {
+        if (source_terms<false>(G, phv, g, i, j, k, dU, q, 0)) book(G, NF_GAMMA_CALC, i, j, k);
+      }
     }
     update_zone(G, i, j, k, Dt, dU, U);
     msum += U[0];
@@ -596,7 +617,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_C2P_MINB) k_update_c2p(const __grid
     const int k = HG_NGH + (int)(tq / N1);
     const long o = off3(G, i, j, k);
     Geom gl;
-    if (MDIM != 0) load_geom(G, 3, i, j, gl);
+    if (MDIM != 0) load_geom(G, 3, i, j, gl, k, sub + 1);
     const Geom &g = (MDIM == 0) ? G.g0 : gl;
     double U[HG_NPR], pf[HG_NPR];
     // Newton guess: the predictor's p_f (= ph) holds the unscaled copy of p;
@@ -658,12 +679,12 @@ __global__ void __launch_bounds__(HG_BLK, HG_C2P_MINB) k_update_c2p(const __grid
 // them) and the inversions Utoprim_1d_ee / Utoprim_1d_ee2.  pow() of the
 // reference is the correctly rounded hg_cr_pow (hg_crpow.h).
 template <bool RS>
-__device__ __forceinline__ double ee_face_flux(const GridDev &G, const double *p_h, int d, int i, int j, int k)
+__device__ __forceinline__ double ee_face_flux(const GridDev &G, const double *p_h, int d, int i, int j, int k, int slot)
 {
   double pl[HG_NPR], pr[HG_NPR];
   face_prims<RS>(G, p_h, d, i, j, k, pl, pr);
   Geom g;
-  load_geom(G, d, i, j, g);
+  load_geom(G, d, i, j, g, k, slot);
   State ql, qr;
   get_state(pl, g, G.gam, ql);
   get_state(pr, g, G.gam, qr);
@@ -691,7 +712,7 @@ __device__ __forceinline__ double ee_face_flux(const GridDev &G, const double *p
 // thread, ahead of k_fallback: q_F[6 e + f], f = 0..2 the lower faces of
 // x1..x3, 3..5 the upper ones.
 template <bool RS>
-__global__ void __launch_bounds__(HG_BLK, HG_EE_MINB) k_ee_faces(GridDev G, const double *__restrict__ p_h)
+__global__ void __launch_bounds__(HG_BLK, HG_EE_MINB) k_ee_faces(GridDev G, const double *__restrict__ p_h, int slot)
 {
   const long n = 6L * min(G.sc->q_count, (int)G.capacity);
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
@@ -699,20 +720,21 @@ __global__ void __launch_bounds__(HG_BLK, HG_EE_MINB) k_ee_faces(GridDev G, cons
     const int f = (int)(t % 6), d = f % 3, up = f / 3;
     int i, j, k;
     unpack_ijk(G.q_idx[e], i, j, k);
-    G.q_F[t] = ee_face_flux<RS>(G, p_h, d, i + (up && d == 0), j + (up && d == 1), k + (up && d == 2));
+    G.q_F[t] = ee_face_flux<RS>(G, p_h, d, i + (up && d == 0), j + (up && d == 1), k + (up && d == 2), slot);
   }
 }
 
 template <bool RS>
 __device__ __noinline__ int fixup_entropy_eq(const GridDev &G, long e, int i, int j, int k,
                                              const double *prim_old, double *prim, const Geom &geom,
-                                             const double *Un, double Dt, double *gamma_out)
+                                             const Geom &geom_old, const double *Un, double Dt, double *gamma_out)
 {
   double prim_backup[HG_NPR], gamma;
   for (int l = 0; l < HG_NPR; l++) prim_backup[l] = prim[l];
   const double gam = G.gam;
-  gamma_calc(prim_old, geom, &gamma);
-  const double S_old = geom.g * (gam - 1.) * prim_old[UU] * gamma / (geom.alpha * hg_cr_pow(prim_old[RHO], (gam - 1.)));
+  gamma_calc(prim_old, geom_old, &gamma);
+  const double S_old = geom_old.g * (gam - 1.) * prim_old[UU] * gamma /
+                       (geom_old.alpha * hg_cr_pow(prim_old[RHO], (gam - 1.)));
   double Fm[3], Fp[3];
   for (int d = 0; d < 3; d++) {
     Fm[d] = G.q_F[6 * e + d];
@@ -758,8 +780,10 @@ __global__ void __launch_bounds__(HG_BLK) k_fallback(GridDev G, int sub, double 
       pf[l] = (sub == 0 || !RS) ? pold[l] : rs_roundtrip(G, pold[l], l, i);
       pg[l] = pf[l];
     }
-    Geom g;
-    load_geom(G, 3, i, j, g);
+    Geom g, g_old;
+    load_geom(G, 3, i, j, g, k, sub + 1);
+    if (G.mdim == 3) load_geom(G, 3, i, j, g_old, k, 0);  // geom_old of recover_primitives: n_beg
+    else g_old = g;
     double gamma = 0., bsq = 0.;
     int ret = utoprim_2d(U, g, G.gam, pf, &gamma, &bsq);
     if ((!ret) && (check_gamma(gamma) == 2)) {
@@ -793,7 +817,7 @@ __global__ void __launch_bounds__(HG_BLK) k_fallback(GridDev G, int sub, double 
         book(G, NF_UTOPRIM, i, j, k);
       }
       for (int l = 0; l < B1; l++) pf[l] = pg[l];
-      const int ret_ee = fixup_entropy_eq<RS>(G, e, i, j, k, pold, pf, g, U, Dt, &gamma);
+      const int ret_ee = fixup_entropy_eq<RS>(G, e, i, j, k, pold, pf, g, g_old, U, Dt, &gamma);
       if (ret_ee) {
         if (ret) {
           book(G, NF_UTOPRIM_EE, i, j, k);
@@ -886,7 +910,7 @@ __device__ __forceinline__ int inflow_check(double *pr, const Geom &g, int type)
 // a ghost, then the flips if j is a ghost.  A gamma failure in inflow_check
 // is booked only where the reference calls it (j and k physical).
 __device__ __forceinline__ void bounds_spherical3(const GridDev &G, double *__restrict__ pa, int i, int j, int k,
-                                                  long od)
+                                                  long od, int slot)
 {
   const int N0 = G.N[0], N1 = G.N[1], N2 = G.N[2];
   const int si = bc_map(i, N0, 0), sj = sph_reflect(j, N1), sk = bc_map(k, N2, 1);
@@ -896,7 +920,7 @@ __device__ __forceinline__ void bounds_spherical3(const GridDev &G, double *__re
   for (int l = 0; l < HG_NPR; l++) v[l] = pa[l * G.S + os];
   if (i != si) {
     Geom g;
-    load_geom(G, 3, i, sj, g);
+    load_geom(G, 3, i, sj, g, sk, slot);
     if (inflow_check(v, g, i > si ? 1 : 0) && j == sj && k == sk) book(G, NF_GAMMA_CALC, i, j, k);
   }
   if (j != sj) {
@@ -907,7 +931,9 @@ __device__ __forceinline__ void bounds_spherical3(const GridDev &G, double *__re
   for (int l = 0; l < HG_NPR; l++) put_state(G, pa, l * G.S + od, v[l]);
 }
 
-__global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict__ pa, int conditional)
+// slot: the geometry level inflow_check reads (ncurr: n_mid after the
+// predictor, n_end after the corrector; n_beg outside a step)
+__global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict__ pa, int conditional, int slot)
 {
   if (conditional && !G.sc->bnd_phys) return;
   const int T0 = G.T[0], T1 = G.T[1], T2 = G.T[2];
@@ -945,7 +971,7 @@ __global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict
     // degenerate directions have no ghosts, so these are reference indices
     const long od = (long)i * G.st[0] + (long)j * G.st[1] + (long)k * G.st[2];
     if (G.bc == 10) {
-      bounds_spherical3(G, pa, i, j, k, od);
+      bounds_spherical3(G, pa, i, j, k, od, slot);
       G.pflag[od] = fl ? G.pflag[(long)bc_map(i, N0, 0) * G.st[0] + (long)sph_reflect(j, N1) * G.st[1] +
                                  (long)bc_map(k, N2, 1) * G.st[2]]
                        : 0;
@@ -967,7 +993,7 @@ __global__ void __launch_bounds__(HG_BLK) k_bounds(GridDev G, double *__restrict
 // fixup_interp_v / fixup_interp_prim (fixup.c:499-761) over the flagged list.
 // A zone only reads unflagged neighbours, which no thread writes, so the
 // zones are independent and the order of the reference's loop is immaterial.
-__global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict__ pv)
+__global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict__ pv, int slot)
 {
   const int n = min(G.sc->fl_count, (int)G.capacity);
   const long S = G.S;
@@ -996,7 +1022,7 @@ __global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict_
     for (int l = 0; l < HG_NPR; l++) pc[l] = pv[l * S + o];
     for (int l = lo; l <= hi; l++) pold[l] = pc[l];
     Geom g;
-    load_geom(G, 3, i, j, g);
+    load_geom(G, 3, i, j, g, k, slot);
     double gamma, f, gamma_old;
     int i_ret;
     const int ngood_min = ngood_min_tab[G.nsd];
@@ -1039,7 +1065,7 @@ __global__ void __launch_bounds__(HG_BLK) k_fixup(GridDev G, double *__restrict_
           for (int kk = -1; kk <= 1; kk++)
             if ((good >> (13 + ii + 3 * (jj + 3 * kk))) & 1u) {
               Geom g2;
-              load_geom(G, 3, i + ii, j + jj, g2);
+              load_geom(G, 3, i + ii, j + jj, g2, k + kk, slot);
               ci = i + ii;
               cj = j + jj;
               ck = k + kk;
@@ -1114,7 +1140,7 @@ __global__ void __launch_bounds__(HG_BLK) k_fixup_cells(GridDev G)
     const int k = HG_NGH + (int)(tq / N1);
     const long o = off3(G, i, j, k);
     Geom g;
-    if (G.mdim != 0) load_geom(G, 3, i, j, g);
+    if (G.mdim != 0) load_geom(G, 3, i, j, g, k, 0);
     else g = G.g0;
     double pv[HG_NPR];
     for (int l = 0; l < HG_NPR; l++) pv[l] = G.p[l * S + o];
@@ -1183,7 +1209,141 @@ __global__ void k_timestep(GridDev G, int nblk)
 }
 
 // ---------------------------------------------------------------------------
+// metric_dim 3: the time levels of the geometry and the connection.
+
+__device__ __forceinline__ double *dyn_level(const GridDev &G, int slot)
+{
+  const int L = G.sc->lev[slot];
+  return L == 0 ? G.geomL[0] : L == 1 ? G.geomL[1] : G.geomL[2];
+}
+
+// set_general_geometry (metric.c:3390-3499) for the time level `slot`, at
+// t + tfac dx[0] (tfac 0, 0.5, 1 for n_beg, n_mid, n_end; metric.c:405-407,
+// 3681-3683): the struct of_geom of the five positions of every stored zone.
+__global__ void __launch_bounds__(HG_BLK) k_geom_level(GridDev G, int slot, double tfac)
+{
+  double *out = dyn_level(G, slot);
+  const double t = G.sc->t + tfac * G.sc->dt;
+  const unsigned T0 = G.T[0], T1 = G.T[1];
+  const unsigned total = 5u * (unsigned)G.S;  // < 2^31 (hg_init's bound on 5 planes)
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const unsigned pos = e / (unsigned)G.S, o = e - pos * (unsigned)G.S;
+    const int i = (int)(o % T0), j = (int)((o / T0) % T1), k = (int)(o / (T0 * T1));
+    Geom g;
+    dyn_geom(G, (int)pos, i, j, k, t, g);
+    double *w = out + e;
+    const long s = G.gS3;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        w[(a * 4 + b) * s] = g.gcon[a][b];
+        w[(16 + a * 4 + b) * s] = g.gcov[a][b];
+      }
+    w[32 * s] = g.g;
+    w[33 * s] = g.g_inv;
+    w[34 * s] = g.alpha;
+    for (int a = 0; a < 3; a++) w[(35 + a) * s] = g.beta[a];
+    for (int a = 0; a < 4; a++) w[(38 + a) * s] = g.ncon[a];
+  }
+}
+
+// advance_geometry (metric.c:398-430), the rotation: the step's end becomes
+// the next step's start; k_geom_level then fills n_mid and n_end.
+__global__ void k_advance_geometry(DevScalars *sc)
+{
+  const int n = sc->lev[0];
+  sc->lev[0] = sc->lev[2];
+  sc->lev[2] = n;
+}
+
+// gcov of the level `slot` table at (pos, i, j, k), entry (a, b)
+__device__ __forceinline__ double dyn_gcov_at(const GridDev &G, const double *lv, int pos, int i, int j, int k, int a,
+                                              int b)
+{
+  return lv[(16 + a * 4 + b) * G.gS3 + (long)pos * G.S + off3(G, i, j, k)];
+}
+
+// set_general_conn (metric.c:3507-3648) at time t + tfac dx[0] from the
+// level `slot` (ncurr): for every physical zone, conn_func_fd4
+// (metric.c:212-247) -- the time derivative of gcov_func over +-dt_conn
+// (conn.h:8-20), 4th-order differences of the stored gcov in x1, x2, x3
+// (conn.h:44-86, weights invdx/6 and 4 invdx/3), on a physical x2 boundary
+// the one-sided x2 stencils of conn_func_fd4_lo2 / _hi2 (metric.c:254-340,
+// weights metric.c:3526-3540) -- and DGCOV_TO_CONN (conn.h:25-37) with the
+// zone's gcon.  Written to conn3 in conn[a][b][c] order.
+__global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double tfac)
+{
+  const double *lv = dyn_level(G, slot);
+  const double t = G.sc->t + tfac * G.sc->dt;
+  const double dtc = G.dyn.dt_conn, half_inv_dt_conn = 0.5 / dtc;
+  const unsigned N0 = G.N[0], N1 = G.N[1];
+  const unsigned total = (unsigned)G.capacity;
+  const bool phys2 = (G.bc != 1);  // x2 boundaries physical (not periodic)
+  const int N2S = HG_NGH, N2E = G.NE[1];
+  double w1[4], w2[4];
+  for (int d = 1; d < 4; d++) {
+    w1[d] = G.invdx[d] / 6.;
+    w2[d] = 4. * G.invdx[d] / 3.;
+  }
+  const double i2 = G.invdx[2];
+  const double w_2lo[5] = {-0.5 * i2, -5. * i2 / 3., 3. * i2, -i2, i2 / 6.};
+  const double w_2hi[5] = {-i2 / 6., i2, -3. * i2, 5. * i2 / 3., 0.5 * i2};
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const unsigned q = e / N0;
+    const int i = HG_NGH + (int)(e - q * N0), j = HG_NGH + (int)(q % N1), k = HG_NGH + (int)(q / N1);
+    double c[4][4][4];
+    {  // time component
+      double gh[4][4], gl[4][4];
+      dyn_gcov_func(G, 3, i, j, k, t + dtc, gh);
+      dyn_gcov_func(G, 3, i, j, k, t - dtc, gl);
+      for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) c[a][b][0] = (gh[a][b] - gl[a][b]) * half_inv_dt_conn;
+    }
+    for (int a = 0; a < 4; a++)
+      for (int b = 0; b < 4; b++) {
+        // x1: CENT i-1, FACE1 i, FACE1 i+1, CENT i+1
+        c[a][b][1] = w1[1] * (dyn_gcov_at(G, lv, 3, i - 1, j, k, a, b) - dyn_gcov_at(G, lv, 3, i + 1, j, k, a, b)) +
+                     w2[1] * (dyn_gcov_at(G, lv, 0, i + 1, j, k, a, b) - dyn_gcov_at(G, lv, 0, i, j, k, a, b));
+        if (phys2 && j == N2S) {
+          c[a][b][2] = w_2lo[0] * dyn_gcov_at(G, lv, 1, i, j, k, a, b) + w_2lo[1] * dyn_gcov_at(G, lv, 3, i, j, k, a, b) +
+                       w_2lo[2] * dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b) +
+                       w_2lo[3] * dyn_gcov_at(G, lv, 3, i, j + 1, k, a, b) +
+                       w_2lo[4] * dyn_gcov_at(G, lv, 1, i, j + 2, k, a, b);
+        } else if (phys2 && j == N2E) {
+          c[a][b][2] = w_2hi[0] * dyn_gcov_at(G, lv, 1, i, j - 1, k, a, b) +
+                       w_2hi[1] * dyn_gcov_at(G, lv, 3, i, j - 1, k, a, b) + w_2hi[2] * dyn_gcov_at(G, lv, 1, i, j, k, a, b) +
+                       w_2hi[3] * dyn_gcov_at(G, lv, 3, i, j, k, a, b) + w_2hi[4] * dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b);
+        } else {
+          c[a][b][2] = w1[2] * (dyn_gcov_at(G, lv, 3, i, j - 1, k, a, b) - dyn_gcov_at(G, lv, 3, i, j + 1, k, a, b)) +
+                       w2[2] * (dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b) - dyn_gcov_at(G, lv, 1, i, j, k, a, b));
+        }
+        c[a][b][3] = w1[3] * (dyn_gcov_at(G, lv, 3, i, j, k - 1, a, b) - dyn_gcov_at(G, lv, 3, i, j, k + 1, a, b)) +
+                     w2[3] * (dyn_gcov_at(G, lv, 2, i, j, k + 1, a, b) - dyn_gcov_at(G, lv, 2, i, j, k, a, b));
+      }
+    double tmp[4][4][4];
+    for (int a = 0; a < 4; a++)
+      for (int b = 0; b < 4; b++)
+        for (int cc = 0; cc < 4; cc++) tmp[a][b][cc] = 0.5 * (c[b][a][cc] + c[cc][a][b] - c[cc][b][a]);
+    const long o = off3(G, i, j, k);
+    const long oc = 3 * G.S + o;
+    for (int a = 0; a < 4; a++)
+      for (int b = 0; b < 4; b++)
+        for (int cc = 0; cc < 4; cc++) {
+          double v = 0.;
+          for (int l = 0; l < 4; l++) v += lv[(a * 4 + l) * G.gS3 + oc] * tmp[l][b][cc];
+          G.conn3[((a * 4 + b) * 4 + cc) * G.S + o] = v;
+        }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host-side launch sequence of one step.
+static void launch_geom_level(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int slot, double tfac)
+{
+  k_geom_level<<<L.grid_upd, HG_BLK, 0, s>>>(G, slot, tfac);
+}
+
 static inline void mark(EventRec *r, int cls, cudaStream_t s)
 {
   if (!r || r->n >= r->cap) return;
@@ -1245,7 +1405,7 @@ static void launch_strip(const GridDev &G, const LaunchCfg &L, cudaStream_t s, c
 }
 
 static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, int d,
-                            EventRec *R)
+                            EventRec *R, int slot)
 {
     int lo[3], n[3];
     unsigned int mult = 1;
@@ -1270,7 +1430,8 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
       launch_flux_f32(G, L, s, d, lo, n, mult);  // reads G.p32, filled from ph
       return;
     }
-#define HG_FLUX(RSV, MD, DD) k_flux<RSV, MD, DD><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
+#define HG_FLUX(RSV, MD, DD) \
+  k_flux<RSV, MD, DD><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult, slot)
 #define HG_STRIP(RSV, MD, DD) \
   launch_strip<RSV, MD, DD>(G, L, s, ph, lo, n, mult)
 #define HG_FLUX_D(RSV, MD) \
@@ -1280,6 +1441,16 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
     if (G.mdim == 0) {
       if (G.rescale) { HG_FLUX_D(true, 0) }
       else { HG_FLUX_D(false, 0) }
+    } else if (G.mdim == 3) {  // one face per thread, geometry of time level `slot`
+      if (G.rescale) {
+        if (d == 0) HG_FLUX(true, 3, 0);
+        else if (d == 1) HG_FLUX(true, 3, 1);
+        else HG_FLUX(true, 3, 2);
+      } else {
+        if (d == 0) HG_FLUX(false, 3, 0);
+        else if (d == 1) HG_FLUX(false, 3, 1);
+        else HG_FLUX(false, 3, 2);
+      }
     } else {
       if (G.rescale) { HG_FLUX_D(true, 2) }
       else { HG_FLUX_D(false, 2) }
@@ -1296,8 +1467,11 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
   const double dtfac = sub == 0 ? 0.5 : 1.0;
   mark(R, KC_MISC, s);
   k_begin<<<1, 1, 0, s>>>(G.sc);
+  // set_general_conn(t) before the predictor, set_general_conn(t + dx[0]/2)
+  // before the corrector (step_ch.c:79-83, 128-133), from ncurr's level
+  if (G.mdim == 3) k_conn_dyn<<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, 0.5 * sub);
   // (the mixed form's FP32 copy of ph is already current: put_state)
-  for (int d = 0; d < 3; d++) launch_flux_dir(G, L, s, ph, d, R);
+  for (int d = 0; d < 3; d++) launch_flux_dir(G, L, s, ph, d, R, sub);
   {
     int lo[3], n[3];
     for (int a = 0; a < 3; a++) {
@@ -1314,6 +1488,9 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
   if (G.mdim == 0) {
     if (G.rescale) { HG_UPD(true, 0); }
     else { HG_UPD(false, 0); }
+  } else if (G.mdim == 3) {
+    if (G.rescale) { HG_UPD(true, 3); }
+    else { HG_UPD(false, 3); }
   } else {
     if (G.rescale) { HG_UPD(true, 2); }
     else { HG_UPD(false, 2); }
@@ -1321,17 +1498,17 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
 #undef HG_UPD
   mark(R, KC_FALLBACK, s);
   if (G.use_ee) {
-    if (G.rescale) k_ee_faces<true><<<L.grid_fix * 6, HG_BLK, 0, s>>>(G, ph);
-    else k_ee_faces<false><<<L.grid_fix * 6, HG_BLK, 0, s>>>(G, ph);
+    if (G.rescale) k_ee_faces<true><<<L.grid_fix * 6, HG_BLK, 0, s>>>(G, ph, sub);
+    else k_ee_faces<false><<<L.grid_fix * 6, HG_BLK, 0, s>>>(G, ph, sub);
   }
   if (G.rescale) k_fallback<true><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
   else k_fallback<false><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
   mark(R, KC_BOUNDS, s);
-  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, pf, 0);
+  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, pf, 0, sub + 1);
   mark(R, KC_FIXUP, s);
-  k_fixup<<<L.grid_fix, HG_BLK, 0, s>>>(G, pf);
+  k_fixup<<<L.grid_fix, HG_BLK, 0, s>>>(G, pf, sub + 1);
   mark(R, KC_BOUNDS, s);
-  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, pf, 1);
+  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, pf, 1, sub + 1);
 }
 
 __global__ void k_reset_max(DevScalars *sc, int dim) { sc->maxs[dim] = 0ull; }
@@ -1469,14 +1646,14 @@ void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int 
 {
   k_reset_max<<<1, 1, 0, s>>>(G.sc, d + 1);
   if (G.prec == HG_PREC_MIXED) launch_to_f32(G, L.grid_upd, s, G.p);
-  launch_flux_dir(G, L, s, G.p, d, nullptr);
+  launch_flux_dir(G, L, s, G.p, d, nullptr, 0);
 }
 
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
 {
   k_begin<<<1, 1, 0, s>>>(G.sc);
   k_fixup_cells<<<L.grid_upd, HG_BLK, 0, s>>>(G);
-  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0);
+  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0, 0);
   if (G.p32) launch_to_f32(G, L.grid_upd, s, G.p);  // the FP32 copy of the state set from the host
 }
 
@@ -1520,7 +1697,11 @@ __device__ __forceinline__ double divb_zone(const GridDev &G, int i, int j, int 
         const long o = off3(G, i + di, j + dj, k + dk);
         double g;
         if (G.mdim == 0) g = G.g0.g;
-        else g = G.geomT[32 * G.gS + ((long)3 * G.T[1] + (G.deg[1] ? 0 : j + dj)) * G.T[0] + (G.deg[0] ? 0 : i + di)];
+        else if (G.mdim == 3) {
+          const int L = G.sc->lev[0];
+          g = (L == 0 ? G.geomL[0] : L == 1 ? G.geomL[1] : G.geomL[2])[32 * G.gS3 + 3 * G.S + o];
+        } else
+          g = G.geomT[32 * G.gS + ((long)3 * G.T[1] + (G.deg[1] ? 0 : j + dj)) * G.T[0] + (G.deg[0] ? 0 : i + di)];
         const double b1 = G.p[B1 * G.S + o], b2 = G.p[B2 * G.S + o], b3 = G.p[B3 * G.S + o];
         f[0] += (di == 0 ? b1 : -b1) * g;
         f[1] += (dj == 0 ? b2 : -b2) * g;
@@ -1628,7 +1809,7 @@ void *gather_times_kernel() { return (void *)k_gather_times; }
 void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
 {
   k_begin<<<1, 1, 0, s>>>(G.sc);
-  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0);
+  k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, G.p, 0, 0);
   if (G.p32) launch_to_f32(G, L.grid_upd, s, G.p);
 }
 
@@ -1638,7 +1819,20 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
   launch_substep(G, L, s, 1, R);
   mark(R, KC_MISC, s);
   k_timestep<<<1, 1024, 0, s>>>(G, L.grid_upd);
+  if (G.mdim == 3) {  // advance_geometry() at the end of step_ch() (step_ch.c:225-227)
+    k_advance_geometry<<<1, 1, 0, s>>>(G.sc);
+    launch_geom_level(G, L, s, 1, 0.5);
+    launch_geom_level(G, L, s, 2, 1.0);
+  }
   mark(R, KC_END, s);
+}
+
+// all three time levels at t (init_general_metric, metric.c:3664-3690)
+void launch_geom_levels(const GridDev &G, const LaunchCfg &L, cudaStream_t s)
+{
+  launch_geom_level(G, L, s, 0, 0.0);
+  launch_geom_level(G, L, s, 1, 0.5);
+  launch_geom_level(G, L, s, 2, 1.0);
 }
 
 }  // namespace HG_KNS

@@ -36,18 +36,28 @@ __device__ __forceinline__ int off3(const GridDev &G, int i, int j, int k)  // 3
   return i * G.st[0] + j * G.st[1] + k * G.st[2];
 }
 
-// get_geometry (macros.h:605) for the static metrics: metric_dim 0 uses one
-// struct, metric_dim 2 the (pos,i,j) tables.
-__device__ __forceinline__ void load_geom(const GridDev &G, int pos, int i, int j, Geom &g)
+// get_geometry (macros.h:605): metric_dim 0 uses one struct, metric_dim 2
+// the (pos,i,j) tables, metric_dim 3 the (pos,i,j,k) table of time level
+// `slot` (0 n_beg, 1 n_mid, 2 n_end; the buffer of each level is in
+// DevScalars::lev, rotated on the device every step).
+__device__ __forceinline__ void load_geom(const GridDev &G, int pos, int i, int j, Geom &g, int k = 0, int slot = 0)
 {
   if (G.mdim == 0) {
     g = G.g0;
     return;
   }
-  const int ii = G.deg[0] ? 0 : i, jj = G.deg[1] ? 0 : j;
-  const long o = ((long)pos * G.T[1] + jj) * G.T[0] + ii;
-  const double *t = G.geomT + o;
-  const long s = G.gS;
+  const double *t;
+  long s;
+  if (G.mdim == 3) {
+    const int L = G.sc->lev[slot];
+    t = (L == 0 ? G.geomL[0] : L == 1 ? G.geomL[1] : G.geomL[2]) + (long)pos * G.S + off3(G, i, j, k);
+    s = G.gS3;
+  } else {
+    const int ii = G.deg[0] ? 0 : i, jj = G.deg[1] ? 0 : j;
+    const long o = ((long)pos * G.T[1] + jj) * G.T[0] + ii;
+    t = G.geomT + o;
+    s = G.gS;
+  }
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll

@@ -56,8 +56,9 @@ typedef struct hg_grid_desc {
   int32_t use_flux_ct_para;     /* USE_FLUX_CT_PARA (options.h:165) */
   int32_t bc_type;              /* BC_TYPE_CHOICE: 0 CARTESIAN_OUTFLOW, 1 CARTESIAN_PERIODIC,
                                    10 SPHERICAL_OUTFLOW3 (options.h:98-124) */
-  int32_t metric_dim;           /* METRIC_DIM: 0 (one geometry for every cell) or 2
-                                   (axisymmetric tables over i,j) (macros.h:47-53) */
+  int32_t metric_dim;           /* METRIC_DIM: 0 (one geometry for every cell), 2
+                                   (axisymmetric tables over i,j) (macros.h:47-53), or 3
+                                   (time-dependent metric: hg_set_dynamic_metric) */
   int32_t use_entropy_eq;       /* USE_ENTROPY_EQ (options.h:209) */
   int32_t cooling;              /* USE_COOLING_FUNCTION: 0 or 1 (options.h:192) */
   int32_t rescale_r;            /* RESCALE_R (options.h:267) */
@@ -96,6 +97,34 @@ int hg_set_cell_data(hg_handle *h, const double *cell6, const double *rface);
  * cooling_func_hr_disk() tabulates on its first call (phys.c:683-704,
  * omega_circular_equatorial() and target_temperature()). */
 int hg_set_cooling_tables(hg_handle *h, const double *omega, const double *t_target);
+
+/* metric_dim 3: the time-dependent metric path of the reference
+ * (METRIC_GENERAL_DYNAMIC, options.h:79; metric.c:3390-3690).  Its geometry
+ * is not uploaded: the library evaluates it on the device at the step's
+ * three time levels n_beg, n_mid, n_end (set_general_geometry for each,
+ * rotated every step as advance_geometry does, metric.c:398-430) and
+ * rebuilds the connection before every substep by 4th-order differences of
+ * gcov and the time difference of gcov over +-dt_conn (set_general_conn,
+ * metric.c:3507-3648, conn.h).  The spacetime and its COORD_DIAGONAL3
+ * coordinates (coord.c:270-276, set_special_coord of the setup) are
+ * described here.  Spacetimes: HG_DYN_MINK_SPHERICAL, the reference's
+ * METRIC_DYNAMIC_MINK_SPHERICAL test spacetime (options.h:90).  Every
+ * direction must be resolved (N > 1); FP64 forms only. */
+#define HG_DYN_MINK_SPHERICAL 2
+typedef struct hg_dyn_metric {
+  int32_t spacetime;            /* HG_DYN_* */
+  int32_t diag3_exponent;       /* COORD_DIAGONAL3: odd, >= 3 */
+  double R0, h_slope, diag3_factor;
+  double dt_conn;               /* main.c:569 sets 9e-6 */
+} hg_dyn_metric;
+int hg_set_dynamic_metric(hg_handle *h, const hg_dyn_metric *m);
+/* The struct of_geom (HG_NGEOM doubles, hg_set_geometry's order) of position
+ * pos (0..2 FACE1..FACE3, 3 CENT, 4 CORN) of zone (i, j, k) at time t, as the
+ * device evaluates it, computed on the host: for checking the evaluation
+ * against the reference's own tables.  The host's elementary functions
+ * (exp, sincos, pow) are glibc's, the device's CUDA's. */
+int hg_dyn_geometry(const hg_grid_desc *desc, const hg_dyn_metric *m, int32_t pos, int32_t i, int32_t j, int32_t k,
+                    double t, double geom[HG_NGEOM]);
 
 /* Primitive variables in the reference layout (flattened p[i][j][k][l]).
  * Upload is hg_upload_prims; download is what diag()/restart_write() need. */

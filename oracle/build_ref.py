@@ -108,6 +108,18 @@ CONFIGS = {
                ("rmax = 16. ;", "rmax = 12. ;"),
                ("  randfact = 0.;", "  randfact = 4.e-2;"),
                ("phys.c", "const double h_o_r  = 5.e-2;", "const double h_o_r  = 1.e-1;")]),
+    # The torus configuration on the reference's general time-dependent metric
+    # path (METRIC_GENERAL_DYNAMIC: geometry at three time levels, METRIC_DIM
+    # 3 tables, connection rebuilt every substep by 4th-order differences of
+    # gcov plus a time derivative; metric.c:3390-3648, conn.h) with its
+    # Minkowski-spherical test spacetime (METRIC_DYNAMIC_MINK_SPHERICAL,
+    # options.h:90).  SET_TSHRINK 1: main.c:505-508 refuses to compile the
+    # dynamic path without it for every spacetime but the PN ones.
+    "torus_dynmink": ("init.torus.c",
+                      dict(USE_COOLING_FUNCTION="(1)", FLUX_TYPE_CHOICE="(FLUX_HLLE)",
+                           METRIC_TYPE_CHOICE="(METRIC_GENERAL_DYNAMIC)",
+                           METRIC_DYNAMIC_TYPE_CHOICE="(METRIC_DYNAMIC_MINK_SPHERICAL)", SET_TSHRINK="(1)"),
+                      None),
     # Advected field loop (Gardiner & Stone 2005), 2D periodic Minkowski:
     # PPM_MC + HLLE + para flux-CT, the shipped parameters.  The setup calls
     # the time-dependent-coordinate macro SET_GEOM_COORD_TIME_FUNCS without
@@ -123,6 +135,10 @@ CONFIGS = {
                         RECON_TYPE_CHOICE="(RECON_PPM_VL)", FLUX_TYPE_CHOICE="(FLUX_LF)"),
                    []),
 }
+
+
+# the dynamic-metric torus takes the torus configuration's edits of init.torus.c and phys.c
+CONFIGS["torus_dynmink"] = CONFIGS["torus_dynmink"][:2] + (CONFIGS["torus"][2],)
 
 
 def set_define(text, name, value):

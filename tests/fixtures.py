@@ -10,8 +10,20 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CHAOTIC = {"torus_24x16x8_s200"}
 
 
-def names():
+def _all():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def names():
+    """Fixtures of the static metrics (METRIC_DIM 0 and 2), which the C oracle
+    restates too."""
+    return [n for n in _all() if "_dyn" not in n]
+
+
+def dynamic_names():
+    """Fixtures of the time-dependent metric path (METRIC_DIM 3): compared
+    with the engine directly (tests/test_dynamic_metric.py)."""
+    return [n for n in _all() if "_dyn" in n]
 
 
 def load(name):

@@ -53,6 +53,11 @@ CASES = [
     ("balsara1_n1024_tfinal", "balsara1", (1024, 1, 1), "final", None),
     ("linwave_2d_32x32x1_tfinal", "linwave", (32, 32, 1), "final", None),
     ("torus_24x16x8_s200", "torus", (24, 16, 8), 200, "load"),
+    # the torus on the time-dependent metric path (METRIC_GENERAL_DYNAMIC) with
+    # the Minkowski-spherical test spacetime: 3D geometry at three time levels,
+    # connection by 4th-order differences every substep
+    ("torus_dynmink_12x10x6_s1", "torus_dynmink", (12, 10, 6), 1, "load"),
+    ("torus_dynmink_12x10x6_s3", "torus_dynmink", (12, 10, 6), 3, "load"),
 ]
 
 # Runs long enough for the flow to amplify a one-ulp change of pow() to O(1):

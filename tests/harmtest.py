@@ -30,6 +30,7 @@ CONFIG_SWITCHES = {
     "linwave_noee": dict(recon=5, flux=1, ct_para=1, bc=1, metric_dim=0, ee=0, cooling=0, rescale=0),
     "torus": dict(recon=5, flux=1, ct_para=1, bc=10, metric_dim=2, ee=1, cooling=1, rescale=1),
     "field_loop": dict(recon=5, flux=1, ct_para=1, bc=1, metric_dim=0, ee=1, cooling=0, rescale=0),
+    "torus_dynmink": dict(recon=5, flux=1, ct_para=1, bc=10, metric_dim=3, ee=1, cooling=1, rescale=1),
 }
 CONFIG_HOR = 0.1  # h_o_r of the torus build's cooling function
 

@@ -40,7 +40,7 @@ def test_init_rejects_unsupported_switches():
     lib = hg.load_library()
     base = dict(n=(8, 8, 8), gam=4 / 3, cour=0.4, dx=[1e-5, .1, .1, .1], startx=[0, -.3, -.3, -.3],
                 grid_length=[1, 1, 1, 1])
-    bad = [dict(recon=7), dict(flux=3), dict(bc=5), dict(metric_dim=3), dict(n=(0, 8, 8)),
+    bad = [dict(recon=7), dict(flux=3), dict(bc=5), dict(metric_dim=4), dict(metric_dim=3, n=(8, 8, 1)), dict(n=(0, 8, 8)),
            dict(metric_dim=2, n=(8, 1, 8)), dict(rescale_r=1, n=(1, 8, 8)), dict(gam=1.0),
            dict(n=(1290, 1290, 1290))]  # 2^31 entries per plane: past the kernels' 32-bit indexing
     for b in bad:

@@ -1,0 +1,121 @@
+"""The time-dependent metric path (metric_dim 3; the reference's
+METRIC_GENERAL_DYNAMIC) against the reference's own build of it.
+
+Fixtures (tests/golden/make_golden.py, reference configuration
+torus_dynmink of oracle/build_ref.py): the magnetised torus setup on the
+dynamic path with the reference's Minkowski-spherical test spacetime,
+12x10x6 zones, 1 and 3 steps from the reference's own initial data.  The
+reference keeps the geometry of three time levels in 3D tables (METRIC_DIM
+3), rotates them every step and rebuilds the connection before every
+substep by 4th-order differences of gcov (metric.c:3390-3690, conn.h).  The
+engine evaluates the same geometry on the device (k_geom_level, k_conn_dyn).
+
+  * On the host, the evaluation code (hg_dyn_geometry, compiled from the
+    same source as the device kernels) reproduces the reference's tables
+    bit for bit at all five positions of every zone.
+  * On the GPU the elementary functions of that code (exp, sincos, pow) are
+    CUDA's, which round differently from glibc's in the last bit, and the
+    entropy fix uses the correctly rounded pow (tests/test_crpow.py), so
+    the step is compared with a tolerance: primitives within 1e-12 of each
+    variable's largest magnitude after one step and 1e-10 after three, with
+    pflag and every failure counter exactly equal.
+"""
+import numpy as np
+import pytest
+
+import coolharm3d_b200 as hg
+import fixtures
+import harmtest as ht
+
+NAMES = fixtures.dynamic_names()
+
+
+def desc_of(f, precision=hg.PREC_FP64):
+    sw = f["sw"]
+    return hg.make_desc(f["n"], f["gam"], f["cour"], f["dx"], f["startx"], f["grid_length"], t=f["t0"],
+                        recon=sw["recon"], flux=sw["flux"], ct_para=sw["ct_para"], bc=sw["bc"], metric_dim=3,
+                        use_ee=sw["ee"], cooling=sw["cooling"], rescale_r=sw["rescale"], precision=precision)
+
+
+def test_fixtures_are_the_dynamic_path():
+    assert NAMES
+    for name in NAMES:
+        f = fixtures.load(name)
+        n = f["n"]
+        assert f["sw"]["metric_dim"] == 3
+        assert f["geom"].shape == (5 * (n[0] + 6) * (n[1] + 6) * (n[2] + 6), 42)
+        assert f["conn"].shape == (n[0] * n[1] * n[2], 64)
+
+
+def test_host_evaluation_matches_reference_tables():
+    f = fixtures.load(NAMES[0])
+    n = f["n"]
+    T = [x + 6 for x in n]
+    d = desc_of(f)
+    m = hg.dyn_metric()
+    ref = f["geom"]
+    for pos in range(5):
+        for i in range(T[0]):
+            for j in range(T[1]):
+                for k in (0, 2, 5, T[2] - 1):
+                    g = hg.dyn_geometry(d, m, pos, i, j, k, f["t0"])
+                    r = ref[k + T[2] * (j + T[1] * (i + T[0] * pos))]
+                    assert np.array_equal(g, r), (pos, i, j, k)
+
+
+def test_init_refuses_unsupported_dynamic_grids():
+    f = fixtures.load(NAMES[0])
+    lib = hg.load_library()
+    import ctypes
+    for kw in (dict(n=(12, 10, 1)), dict(precision=hg.PREC_MIXED)):
+        n = kw.get("n", f["n"])
+        d = hg.make_desc(n, f["gam"], f["cour"], f["dx"], f["startx"], f["grid_length"], metric_dim=3, bc=10,
+                         precision=kw.get("precision", hg.PREC_FP64))
+        h = ctypes.c_void_p()
+        assert lib.hg_init(ctypes.byref(d), ctypes.byref(h)) == -2, kw
+
+
+def engine_for(f, precision=hg.PREC_FP64):
+    e = hg.Engine(desc_of(f, precision))
+    e.set_dynamic_metric(hg.dyn_metric())
+    e.set_cell_data(fixtures.cell6_of(f), f["rface"])
+    e.set_cooling_tables(f["cool_omega"], f["cool_temp"])
+    e.upload(f["p0"])
+    e.set_time(f["t0"], f["dt0"])
+    return e
+
+
+def normwise_rel(a, b):
+    scale = np.abs(b).reshape(-1, 8).max(0)
+    return np.abs(a - b).reshape(-1, 8).max(0) / np.where(scale > 0, scale, 1.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_engine_matches_reference_dynamic_metric(name):
+    f = fixtures.load(name)
+    e = engine_for(f)
+    t, dt = e.step(f["steps"])
+    n = f["n"]
+    d = normwise_rel(ht.interior(e.download(), n), ht.interior(f["p"], n))
+    print(name, "normwise relative difference per variable", d)
+    assert d.max() <= (1e-12 if f["steps"] == 1 else 1e-10)
+    assert np.array_equal(e.pflag(), f["pflag"])
+    assert e.fail_counts().tolist() == f["nfailtot"].tolist()
+    assert abs(t - f["t"]) <= 1e-15 * f["t"] and abs(dt - f["dt"]) <= 1e-12 * f["dt"]
+    e.close()
+
+
+@pytest.mark.gpu
+def test_dynamic_steps_in_one_call_equal_steps_one_by_one():
+    """The time levels rotate on the device inside each step's graph: three
+    steps at once and three single steps give the same state."""
+    f = fixtures.load(NAMES[0])
+    a = engine_for(f)
+    a.step(3)
+    b = engine_for(f)
+    for _ in range(3):
+        b.step(1)
+    assert np.array_equal(a.download(), b.download())
+    a.close()
+    b.close()
