@@ -76,6 +76,10 @@ WORKLOADS = {
                            "Gamma 5/3, beta 100 loop, H/R 0.1 cooling, PPM_MC+HLLE+para flux-CT, entropy fix, FP64"),
     "torus96": dict(kind="torus", n=(96, 96, 64), ref_cfg="torus",
                     label="Fishbone-Moncrief torus as torus192 on 96x96x64 zones"),
+    "torus192dyn": dict(kind="torus_dyn", n=(192, 192, 128), ref_cfg="torus_dynmink",
+                        label="torus192's initial state on the time-dependent metric path (metric_dim 3): the "
+                              "Minkowski-spherical test spacetime, geometry of three time levels and the "
+                              "finite-difference connection evaluated on the device every step, FP64"),
     "balsara1024": dict(kind="setup", setup="balsara1", n=(1024, 1, 1), ref_cfg="balsara1",
                         label="Balsara-1 shock tube, 1024 zones, MC + HLLE + para flux-CT, CFL 0.5, FP64"),
     "fieldloop512": dict(kind="setup", setup="field_loop", n=(512, 512, 1), ref_cfg="field_loop",
@@ -195,6 +199,20 @@ def setup(wl, device, precision=0, p_init=None):
     uploaded instead of a freshly built initial state."""
     import coolharm3d_b200 as hg
     n = wl["n"]
+    if wl["kind"] == "torus_dyn":
+        from coolharm3d_b200 import torus
+        ks, p0 = setup(dict(wl, kind="torus"), device, precision, p_init)
+        ks.close()
+        desc = torus.torus_desc(n, device=device, precision=precision)
+        t = torus.torus_tables(desc)
+        desc.metric_dim = 3
+        e = hg.Engine(desc)
+        e.set_dynamic_metric(hg.dyn_metric())
+        e.set_cell_data(t["cell6"], t["rface"])
+        e.set_cooling_tables(t["cool_omega"], t["cool_temp"])
+        e.upload(p0)
+        e.set_time(desc.t, desc.dx[0])
+        return e, p0
     if wl["kind"] == "torus":
         from coolharm3d_b200 import torus
         desc = torus.torus_desc(n, device=device, precision=precision)

@@ -52,16 +52,19 @@ void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src
 namespace HG_KNS {
 using namespace hg;
 
-// register caps of the two update kernels (4 blocks of 128 threads per SM;
-// measured best of 1-6 blocks on the torus)
+// register caps (minimum resident blocks of 128 threads per SM), measured on
+// the 192x192x128 torus: the flux and conserved-update kernels at 3 blocks
+// (168 registers, no spills; at 4 blocks, 128 registers, the flux kernels
+// spilled ~3e6 local-load sectors per launch: 6.36 against 6.70 ms per step),
+// the inversion at 4 (118 registers; 3 blocks spilled and measured slower)
 #ifndef HG_CONS_MINB
-#define HG_CONS_MINB 4
+#define HG_CONS_MINB 3
 #endif
 #ifndef HG_C2P_MINB
 #define HG_C2P_MINB 4
 #endif
 #ifndef HG_FLUX_MINB
-#define HG_FLUX_MINB 4
+#define HG_FLUX_MINB 3
 #endif
 #ifndef HG_EE_MINB
 #define HG_EE_MINB 4
