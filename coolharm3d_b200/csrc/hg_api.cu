@@ -48,10 +48,16 @@ void launch_face_flux(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t
 cudaError_t prepare_kernels();
 }  // namespace hg_fma
 
-// one step's launch sequence of the grid's precision form
+// One step's launch sequence of the grid's precision form.  The plain FP64
+// form runs the kernels built without contracted multiply-adds
+// (bit-identical to the reference); the FMA form and the mixed form, whose
+// FP32 fluxes are not bit-identical anyway, run the build with fused
+// multiply-adds for their FP64 kernels.
+static bool fma_kernels(const hg::GridDev &G) { return G.prec == HG_PREC_FP64_FMA || G.prec == HG_PREC_MIXED; }
+
 static void launch_grid_step(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s, hg::EventRec *R)
 {
-  if (G.prec == HG_PREC_FP64_FMA) hg_fma::launch_step(G, L, s, R);
+  if (fma_kernels(G)) hg_fma::launch_step(G, L, s, R);
   else hg::launch_step(G, L, s, R);
 }
 
@@ -862,7 +868,7 @@ extern "C" int hg_face_flux(hg_handle *h, int32_t dir, double *flux, double *max
     int rc = refresh_levels(h);
     if (rc != HG_OK) return rc;
   }
-  if (G.prec == HG_PREC_FP64_FMA) hg_fma::launch_face_flux(G, h->L, h->stream, dir);
+  if (fma_kernels(G)) hg_fma::launch_face_flux(G, h->L, h->stream, dir);
   else hg::launch_face_flux(G, h->L, h->stream, dir);
   HG_CK(cudaGetLastError());
   HG_CK(cudaStreamSynchronize(h->stream));

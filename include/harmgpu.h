@@ -44,7 +44,8 @@ extern "C" {
 #define HG_NGEOM 42             /* doubles per struct of_geom (globals.h:90-98) */
 
 #define HG_PREC_FP64 0          /* every operation in IEEE double, no FMA: bit-identical to the reference */
-#define HG_PREC_MIXED 1         /* reconstruction + HLL flux in FP32, everything else FP64 */
+#define HG_PREC_MIXED 1         /* reconstruction + HLL flux in FP32, everything else FP64
+                                   (with fused multiply-adds) */
 #define HG_PREC_FP64_FMA 2      /* every operation in IEEE double, multiply-adds fused: within
                                    rounding of HG_PREC_FP64, not bit-identical */
 
