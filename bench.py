@@ -76,6 +76,8 @@ WORKLOADS = {
                            "Gamma 5/3, beta 100 loop, H/R 0.1 cooling, PPM_MC+HLLE+para flux-CT, entropy fix, FP64"),
     "torus96": dict(kind="torus", n=(96, 96, 64), ref_cfg="torus",
                     label="Fishbone-Moncrief torus as torus192 on 96x96x64 zones"),
+    "torus96dyn": dict(kind="torus_dyn", n=(96, 96, 64), ref_cfg="torus_dynmink",
+                       label="torus192dyn on 96x96x64 zones"),
     "torus192dyn": dict(kind="torus_dyn", n=(192, 192, 128), ref_cfg="torus_dynmink",
                         label="torus192's initial state on the time-dependent metric path (metric_dim 3): the "
                               "Minkowski-spherical test spacetime, geometry of three time levels and the "

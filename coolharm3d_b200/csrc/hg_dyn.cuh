@@ -61,13 +61,17 @@ HG_DYN_HD void dyn_coords(const DynMetric &m, const double *xp, double *x, doubl
   x[1] = m.R0 + exp(xp[1]);
   x[2] = 0.5 * M_PI * (1. + m.h_slope * ftmp + m.diag3_factor * pow(ftmp, (double)m.diag3_exponent));
   x[3] = xp[3];
+#pragma unroll
   for (int a = 0; a < 4; a++)
+#pragma unroll
     for (int b = 0; b < 4; b++) dx_dxp[a][b] = (a == b) ? 1. : 0.;
   dx_dxp[1][1] = x[1] - m.R0;
   dx_dxp[2][2] = M_PI * (m.h_slope + m.diag3_exponent * m.diag3_factor * pow(ftmp, (double)(m.diag3_exponent - 1)));
   const double a11 = dx_dxp[1][1], a12 = dx_dxp[1][2], a21 = dx_dxp[2][1], a22 = dx_dxp[2][2];
   const double inv_det = 1. / (a11 * a22 - a12 * a21);
+#pragma unroll
   for (int a = 0; a < 4; a++)
+#pragma unroll
     for (int b = 0; b < 4; b++) dxp_dx[a][b] = (a == b) ? 1. : 0.;
   dxp_dx[1][1] = a22 * inv_det;
   dxp_dx[1][2] = -a12 * inv_det;
@@ -90,12 +94,12 @@ HG_DYN_HD void dyn_trig(double th, double *cth, double *sth)
 // general_gcov_func of the dynamic path (metric.h:165-167) and, for the
 // tables, gcon and sqrt(-g) (mink_spherical_gcov/gcon/gdet_func,
 // metric.c:2015-2095)
-HG_DYN_HD void dyn_gcov_x(const DynMetric &m, const double *x, double gcov[4][4])
+HG_DYN_HD void dyn_gcov_sth(const double *x, double t1, double gcov[4][4])
 {
-  double cth, t1;
-  const double r = x[1], th = x[2];
-  dyn_trig(th, &cth, &t1);
+  const double r = x[1];
+#pragma unroll
   for (int a = 0; a < 4; a++)
+#pragma unroll
     for (int b = 0; b < 4; b++) gcov[a][b] = 0.;
   gcov[0][0] = -1.;
   gcov[1][1] = 1.;
@@ -103,12 +107,21 @@ HG_DYN_HD void dyn_gcov_x(const DynMetric &m, const double *x, double gcov[4][4]
   gcov[3][3] = gcov[2][2] * t1 * t1;
 }
 
-HG_DYN_HD void dyn_gcon_x(const DynMetric &m, const double *x, double gcon[4][4])
+HG_DYN_HD void dyn_gcov_x(const DynMetric &m, const double *x, double gcov[4][4])
 {
-  double cth, t2;
-  const double r = x[1], th = x[2];
-  dyn_trig(th, &cth, &t2);
+  double cth, t1;
+  dyn_trig(x[2], &cth, &t1);
+  dyn_gcov_sth(x, t1, gcov);
+}
+
+// gcon and sqrt(-g) from the same sin(th) (trigvalues is a pure function of
+// th: the reference's three calls return the same value)
+HG_DYN_HD void dyn_gcon_sth(const double *x, double t2, double gcon[4][4])
+{
+  const double r = x[1];
+#pragma unroll
   for (int a = 0; a < 4; a++)
+#pragma unroll
     for (int b = 0; b < 4; b++) gcon[a][b] = 0.;
   const double t1 = r * r, t3 = t2 * t2;
   gcon[0][0] = -1.;
@@ -117,12 +130,7 @@ HG_DYN_HD void dyn_gcon_x(const DynMetric &m, const double *x, double gcon[4][4]
   gcon[3][3] = gcon[2][2] / t3;
 }
 
-HG_DYN_HD double dyn_gdet_x(const DynMetric &m, const double *x)
-{
-  double cth, t1;
-  dyn_trig(x[2], &cth, &t1);
-  return x[1] * x[1] * fabs(t1);
-}
+HG_DYN_HD double dyn_gdet_sth(const double *x, double t1) { return x[1] * x[1] * fabs(t1); }
 
 // The struct of_geom of one position at time t: set_general_geometry's loop
 // body (metric.c:3453-3483) with transform_all (coord.c:2340-2355:
@@ -133,18 +141,28 @@ HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t
   double xp[4], x[4], dx_dxp[4][4], dxp_dx[4][4], det;
   dyn_xp(G, pos, i, j, k, t, xp);
   dyn_coords(m, xp, x, dx_dxp, dxp_dx, &det);
-  double gc[4][4], gn[4][4];
-  dyn_gcov_x(m, x, gc);
-  dyn_gcon_x(m, x, gn);
-  g.g = dyn_gdet_x(m, x);
+  double gc[4][4], gn[4][4], cth, sth;
+  dyn_trig(x[2], &cth, &sth);
+  dyn_gcov_sth(x, sth, gc);
+  dyn_gcon_sth(x, sth, gn);
+  g.g = dyn_gdet_sth(x, sth);
+  // The sums of transform_rank2cov2/con2 in their order, leaving out the
+  // terms whose Jacobian factor is exactly zero (most of them: COORD_DIAGONAL3
+  // couples only r-x1 and th-x2); adding those zero products changes no sum.
+#pragma unroll
   for (int ip = 0; ip < 4; ip++)
+#pragma unroll
     for (int jp = 0; jp < 4; jp++) {
       double c = 0., n = 0.;
-      for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const double ja = dx_dxp[a][ip], ka = dxp_dx[ip][a];
+#pragma unroll
         for (int b = 0; b < 4; b++) {
-          c += gc[a][b] * dx_dxp[a][ip] * dx_dxp[b][jp];
-          n += gn[a][b] * dxp_dx[ip][a] * dxp_dx[jp][b];
+          if (ja != 0. && dx_dxp[b][jp] != 0.) c += gc[a][b] * ja * dx_dxp[b][jp];
+          if (ka != 0. && dxp_dx[jp][b] != 0.) n += gn[a][b] * ka * dxp_dx[jp][b];
         }
+      }
       g.gcov[ip][jp] = c;
       g.gcon[ip][jp] = n;
     }

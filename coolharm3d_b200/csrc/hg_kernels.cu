@@ -1300,10 +1300,14 @@ __global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double
       double gh[4][4], gl[4][4];
       dyn_gcov_func(G, 3, i, j, k, t + dtc, gh);
       dyn_gcov_func(G, 3, i, j, k, t - dtc, gl);
+#pragma unroll
       for (int a = 0; a < 4; a++)
+#pragma unroll
         for (int b = 0; b < 4; b++) c[a][b][0] = (gh[a][b] - gl[a][b]) * half_inv_dt_conn;
     }
+#pragma unroll
     for (int a = 0; a < 4; a++)
+#pragma unroll
       for (int b = 0; b < 4; b++) {
         // x1: CENT i-1, FACE1 i, FACE1 i+1, CENT i+1
         c[a][b][1] = w1[1] * (dyn_gcov_at(G, lv, 3, i - 1, j, k, a, b) - dyn_gcov_at(G, lv, 3, i + 1, j, k, a, b)) +
@@ -1324,17 +1328,24 @@ __global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double
         c[a][b][3] = w1[3] * (dyn_gcov_at(G, lv, 3, i, j, k - 1, a, b) - dyn_gcov_at(G, lv, 3, i, j, k + 1, a, b)) +
                      w2[3] * (dyn_gcov_at(G, lv, 2, i, j, k + 1, a, b) - dyn_gcov_at(G, lv, 2, i, j, k, a, b));
       }
-    double tmp[4][4][4];
-    for (int a = 0; a < 4; a++)
-      for (int b = 0; b < 4; b++)
-        for (int cc = 0; cc < 4; cc++) tmp[a][b][cc] = 0.5 * (c[b][a][cc] + c[cc][a][b] - c[cc][b][a]);
+    // DGCOV_TO_CONN with tmp[l][b][cc] formed where it is used (the same
+    // operations, without a second 64-entry array per thread)
     const long o = off3(G, i, j, k);
     const long oc = 3 * G.S + o;
+    double gcon[4][4];
+#pragma unroll
     for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int l = 0; l < 4; l++) gcon[a][l] = lv[(a * 4 + l) * G.gS3 + oc];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
       for (int b = 0; b < 4; b++)
+#pragma unroll
         for (int cc = 0; cc < 4; cc++) {
           double v = 0.;
-          for (int l = 0; l < 4; l++) v += lv[(a * 4 + l) * G.gS3 + oc] * tmp[l][b][cc];
+#pragma unroll
+          for (int l = 0; l < 4; l++) v += gcon[a][l] * (0.5 * (c[b][l][cc] + c[cc][l][b] - c[cc][b][l]));
           G.conn3[((a * 4 + b) * 4 + cc) * G.S + o] = v;
         }
   }
