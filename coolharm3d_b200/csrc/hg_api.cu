@@ -78,7 +78,7 @@ struct hg_handle {
   std::vector<void *> allocs;
   double *h_stage = nullptr;  // pinned transfer chunks (HG_XCH x HG_XCH_BYTES)
   cudaEvent_t xev[HG_XCH] = {};  // DMA completion of each transfer chunk
-  double *d_ref = nullptr;    // device buffer in the reference layout, when F[0] is too small
+  double *d_ref = nullptr;    // device buffer in the reference layout (host <-> device transfers)
   cudaGraph_t step_graph = nullptr;  // one hg_step(1) captured (batches, and hg_step itself)
   cudaGraphExec_t step_exec = nullptr;  // step_graph instantiated for hg_step
   bool exec_stale = true;
@@ -476,11 +476,12 @@ extern "C" int hg_set_cooling_tables(hg_handle *h, const double *omega, const do
 // caller's memory and two slots of their own, so host copies overlap one
 // another and the DMA of the other chunks.  On the device the stream lands
 // in a buffer in the same layout, and a kernel converts it to or from the
-// resident planes.  That buffer is F[0] (dead between steps) when the
-// reference layout is no larger than the planes, else a buffer of its own.
+// resident planes.  That buffer is a buffer of its own, allocated on the
+// first transfer: the flux planes are not free between steps, because
+// hg_get_totals (dump_ener's boundary-flux integrals) reads the last
+// substep's fluxes after the driver has brought the primitives back.
 static double *ref_buffer(hg_handle *h)
 {
-  if (h->ntot_ref <= h->G.S) return h->G.F[0];
   if (!h->d_ref) {
     void *q = nullptr;
     if (dev_alloc(h, &q, sizeof(double) * HG_NPR * h->ntot_ref) != HG_OK) return nullptr;
@@ -1275,7 +1276,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
     if (d->rescale_r) b += 4ull * 12 * T[0];
   }
   b += 8ull * 148 * 8;                        // per-block partials
-  if (NT > S) b += 8ull * HG_NPR * NT;        // transfer buffer of a grid with a one-zone direction
+  b += 8ull * HG_NPR * NT;                    // transfer buffer in the reference layout
   *bytes = b;
   return HG_OK;
 }

@@ -1,17 +1,23 @@
 """The drop-in, compiled for real: the reference's own driver (main.c,
-init.balsara1.c, diag.c, restart.c, ...) with the USE_GPU_STEP hooks of
+the init.*.c setup, diag.c, restart.c, ...) with the USE_GPU_STEP hooks of
 coolharm3d_b200/dropin (apply_patch.py + hg_driver.c) linked against
 libharmgpu.so, against the same sources built without the hooks.
 
-Sources: the reference tree staged by oracle/build_ref.py in
-oracle/_ref/balsara1/src (Balsara test 1, MC + HLLE, CFL 0.5), with one
-test-only edit applied to both builds: the final time 0.4 -> 0.015 (52 steps
-on 1024 zones) so the CPU build finishes in seconds.  Both programs run the
-whole driver loop; the GPU program's restart files (restart_write(), the
-ASCII rdump the driver writes every n_restart steps and at the end) must be
-byte for byte the CPU program's, and its energy file (dump_ener every 10
-steps: U and boundary-flux integrals summed on the device, M_tot from the
-device) must agree to 1e-12 (the sums' order differs)."""
+Two configurations staged by oracle/build_ref.py:
+  * balsara1 (Balsara test 1 on 1024 zones, MC + HLLE, CFL 0.5, Minkowski):
+    final time 0.4 -> 0.015 (52 steps);
+  * torus (the magnetised Fishbone-Moncrief torus on 24x16x8 zones:
+    Kerr-Schild a = 0.9 tables and connection handed over by hg_gpu_init,
+    RESCALE_R, H/R cooling tables from HG_DROPIN_H_O_R, entropy fix):
+    final time 10000 -> 5e-3 (19 steps), and the setup's random
+    perturbation of u switched off, because the reference seeds it from the
+    wall clock (ranc.c:37-41) and the two programs must start alike.
+These test-only edits go to both builds.  Both programs run the whole driver
+loop; the GPU program's restart files (restart_write(): the ASCII rdump the
+driver writes every n_restart steps and at the end) must be byte for byte
+the CPU program's, and its energy file (dump_ener every 10 steps: U and
+boundary-flux integrals summed on the device, M_tot from the device) must
+agree to 1e-12 relative, per column group (the sums' order differs)."""
 import os
 import shutil
 import subprocess
@@ -25,33 +31,46 @@ import pytest
 import harmtest as ht
 
 REPO = ht.REPO
-STAGED = REPO / "oracle" / "_ref" / "balsara1" / "src"
 LIBDIR = REPO / "coolharm3d_b200"
 sys.path.insert(0, str(REPO / "coolharm3d_b200" / "dropin"))
 sys.path.insert(0, str(REPO / "oracle"))
 
-pytestmark = pytest.mark.skipif(not STAGED.is_dir(), reason="reference sources not staged (oracle/build_ref.py)")
-
 CFLAGS = ["-O3", "-fcommon", "-ffp-contract=off", "-w"]
-N = (1024, 1, 1)
+
+# configuration -> (grid, init file, test-only edits (regex, replacement), extra GPU-build defines)
+CASES = {
+    "balsara1": ((1024, 1, 1), "init.balsara1.c", [(r"GridLength\[0\] = 0\.4 ;", "GridLength[0] = 0.015 ;")], []),
+    "torus": ((24, 16, 8), "init.torus.c",
+              [(r"GridLength\[0\] = 10000\. ;", "GridLength[0] = 5.e-3 ;"),
+               (r"(?m)^  randfact = 4\.e-2;", "  randfact = 0.;")],
+              ["-DHG_DROPIN_H_O_R=1.e-1"]),
+}
 
 
-def build_pair(work):
+def staged(cfg):
+    return REPO / "oracle" / "_ref" / cfg / "src"
+
+
+def build_pair(work, cfg="balsara1"):
     """(cpu_exe, gpu_exe) built from one patched copy of the staged sources."""
+    import re
     import apply_patch
     import build_ref
+    n, init_file, edits, defines = CASES[cfg]
     src = os.path.join(work, "src")
-    shutil.copytree(STAGED, src)
-    init = os.path.join(src, "init.balsara1.c")
+    shutil.copytree(staged(cfg), src)
+    init = os.path.join(src, init_file)
     text = open(init).read()
-    assert "GridLength[0] = 0.4 ;" in text
-    open(init, "w").write(text.replace("GridLength[0] = 0.4 ;", "GridLength[0] = 0.015 ;", 1))
+    for pat, rep in edits:
+        text, k = re.subn(pat, rep, text, count=1)
+        assert k == 1, pat
+    open(init, "w").write(text)
     apply_patch.apply(src)
-    common = [s for s in build_ref.BASE_SRCS + ["init.balsara1.c"] if s not in ("main.c", "step_ch.c", "diag.c")]
+    common = [s for s in build_ref.BASE_SRCS + [init_file] if s not in ("main.c", "step_ch.c", "diag.c")]
     jobs = []
     for s in common:
         jobs.append((os.path.join(src, s), os.path.join(work, "o_" + s[:-2] + ".o"), []))
-    for variant, extra in (("cpu", []), ("gpu", ["-DUSE_GPU_STEP=1", "-I", str(REPO / "include")])):
+    for variant, extra in (("cpu", []), ("gpu", ["-DUSE_GPU_STEP=1", "-I", str(REPO / "include")] + defines)):
         for s in ("main.c", "step_ch.c", "diag.c", "hg_driver.c"):
             jobs.append((os.path.join(src, s), os.path.join(work, "%s_%s.o" % (variant, s[:-2])), extra))
     procs = [subprocess.Popen(["gcc"] + CFLAGS + ["-I", src] + extra + ["-c", s, "-o", o]) for s, o, extra in jobs]
@@ -68,27 +87,34 @@ def build_pair(work):
     return exes
 
 
-def run(exe, cwd):
+def run(exe, cwd, n):
     os.makedirs(cwd)
-    r = subprocess.run([exe, "1", "1", "1"] + [str(x) for x in N], cwd=cwd, capture_output=True, text=True,
+    r = subprocess.run([exe, "1", "1", "1"] + [str(x) for x in n], cwd=cwd, capture_output=True, text=True,
                        timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     return r.stdout
 
 
-def test_patched_driver_compiles_and_links():
+@pytest.mark.parametrize("cfg", sorted(CASES))
+def test_patched_driver_compiles_and_links(cfg):
     """Both programs build from the patched sources (no GPU needed to link)."""
+    if not staged(cfg).is_dir():
+        pytest.skip("reference sources not staged (oracle/build_ref.py)")
     with tempfile.TemporaryDirectory() as td:
-        cpu, gpu = build_pair(td)
+        cpu, gpu = build_pair(td, cfg)
         assert os.path.exists(cpu) and os.path.exists(gpu)
 
 
 @pytest.mark.gpu
-def test_patched_driver_reproduces_cpu_run():
+@pytest.mark.parametrize("cfg", sorted(CASES))
+def test_patched_driver_reproduces_cpu_run(cfg):
+    if not staged(cfg).is_dir():
+        pytest.skip("reference sources not staged (oracle/build_ref.py)")
+    n = CASES[cfg][0]
     with tempfile.TemporaryDirectory() as td:
-        cpu, gpu = build_pair(td)
-        out_c = run(cpu, os.path.join(td, "run_cpu"))
-        out_g = run(gpu, os.path.join(td, "run_gpu"))
+        cpu, gpu = build_pair(td, cfg)
+        out_c = run(cpu, os.path.join(td, "run_cpu"), n)
+        out_g = run(gpu, os.path.join(td, "run_gpu"), n)
         rc, rg = Path(td, "run_cpu"), Path(td, "run_gpu")
         dumps = sorted(p.name for p in rc.glob("rdump*"))
         assert dumps and dumps == sorted(p.name for p in rg.glob("rdump*"))
@@ -97,7 +123,13 @@ def test_patched_driver_reproduces_cpu_run():
         # the driver's step count and zone-cycles line (main.c:117)
         ns = [line for line in out_c.splitlines() if line.startswith("ns,ts")]
         assert ns and ns == [line for line in out_g.splitlines() if line.startswith("ns,ts")]
-        ec = np.loadtxt(rc / "KDHARM0_ener.out")
-        eg = np.loadtxt(rg / "KDHARM0_ener.out")
-        assert ec.shape == eg.shape
-        np.testing.assert_allclose(eg, ec, rtol=1e-12, atol=1e-15 * np.abs(ec).max())
+        ec = np.loadtxt(rc / "KDHARM0_ener.out", ndmin=2)
+        eg = np.loadtxt(rg / "KDHARM0_ener.out", ndmin=2)
+        assert ec.shape == eg.shape == (ec.shape[0], 3 + 8 + 1 + 48)
+        # nstep, t, dt exactly; then per group (U_tot[8], M_tot, the six
+        # boundary planes' F_tot[8]) relative 1e-12, with 1e-12 of the group's
+        # largest magnitude for sums that cancel to nearly nothing
+        np.testing.assert_array_equal(eg[:, :3], ec[:, :3])
+        for lo, hi in [(3, 11), (11, 12)] + [(12 + 8 * q, 20 + 8 * q) for q in range(6)]:
+            np.testing.assert_allclose(eg[:, lo:hi], ec[:, lo:hi], rtol=1e-12,
+                                       atol=1e-12 * np.abs(ec[:, lo:hi]).max(), err_msg="columns %d-%d" % (lo, hi - 1))

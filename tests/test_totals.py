@@ -45,3 +45,20 @@ def test_device_totals_match_oracle(name):
     assert np.abs(fl - flo).max() <= 1e-11 * scale, (fl, flo)
     assert dmax == pytest.approx(dmo, rel=1e-9, abs=1e-18)
     e.close()
+
+
+@pytest.mark.gpu
+def test_totals_survive_a_download_of_the_primitives():
+    """The driver brings p back before diag() (and so dump_ener) runs: the
+    boundary-flux integrals read after that download are the step's own."""
+    f = fixtures.load("torus_24x16x8_s3")
+    e, _ = engine_for(f["n"], f["sw"], f, f["p0"], f["t0"], f["dt0"])
+    e.step(f["steps"])
+    before = e.totals()
+    e.download()
+    e.pflag()
+    e.gamma()
+    after = e.totals()
+    for a, b in zip(before, after):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    e.close()
