@@ -120,6 +120,36 @@ CONFIGS = {
                            METRIC_TYPE_CHOICE="(METRIC_GENERAL_DYNAMIC)",
                            METRIC_DYNAMIC_TYPE_CHOICE="(METRIC_DYNAMIC_MINK_SPHERICAL)", SET_TSHRINK="(1)"),
                       None),
+    # The circumbinary-disk setup of the post-Newtonian binary runs
+    # (init.nz_pn_bbh_disk.c: De Villiers-Hawley-Krolik disk with q = 1.58
+    # around the binary's total mass M = 1 at separation 20M, inner edge 2(a+M),
+    # pressure maximum 5(a+M), 1% perturbation of u from ranc() seeded with 1,
+    # dipole loop following the density) on the dynamic-metric path.  The PN
+    # spacetime bodies are absent from the reference (metric.h:105-171), so
+    # the reference's own Minkowski-spherical test spacetime stands in for it.
+    # Parameters of the configuration: r over [0.75a, 13a] (Rin 0.05a -> 0.75a,
+    # Rout 100a -> 13a), plasma beta 100 -> 10, H/R = 0.1 cooling (h_o_r 0.05
+    # -> 0.1).  The shipped file does not compile against this source tree;
+    # the four compile fixes, each the evident intent: the two diagnostic
+    # arrays sized by N1TOT at file scope (a run-time size here) get a fixed
+    # size, the local prototype of init_prim() takes the struct of_coord * of
+    # its definition, the diagnostic `rdiskout = x[RR]` reads coords->x[RR],
+    # and get_rpmax()'s coords_loc is the struct of_coord that coord_of_r()
+    # fills (it was declared struct of_geom).
+    "pnbbh_dynmink": ("init.nz_pn_bbh_disk.c",
+                      dict(USE_COOLING_FUNCTION="(1)", FLUX_TYPE_CHOICE="(FLUX_HLLE)",
+                           METRIC_TYPE_CHOICE="(METRIC_GENERAL_DYNAMIC)",
+                           METRIC_DYNAMIC_TYPE_CHOICE="(METRIC_DYNAMIC_MINK_SPHERICAL)", SET_TSHRINK="(1)"),
+                      [("double height_denom[N1TOT] = {0.};", "double height_denom[4096] = {0.};"),
+                       ("double height_numer[N1TOT] = {0.};", "double height_numer[4096] = {0.};"),
+                       ("  void init_prim( int i, int j, int k, double *xp, double *pr);",
+                        "  void init_prim( int i, int j, int k, struct of_coord *coords, double *pr);"),
+                       ("{ rdiskout = x[RR]; }", "{ rdiskout = coords->x[RR]; }"),
+                       ("  struct of_geom coords_loc;", "  struct of_coord coords_loc;"),
+                       ("Rout     = 100.*initial_bbh_separation;", "Rout     = 13.*initial_bbh_separation;"),
+                       ("Rin = 0.05 * (initial_bbh_separation) ;", "Rin = 0.75 * (initial_bbh_separation) ;"),
+                       ("beta     = 1.e2 ;", "beta     = 10. ;"),
+                       ("phys.c", "const double h_o_r  = 5.e-2;", "const double h_o_r  = 1.e-1;")]),
     # Advected field loop (Gardiner & Stone 2005), 2D periodic Minkowski:
     # PPM_MC + HLLE + para flux-CT, the shipped parameters.  The setup calls
     # the time-dependent-coordinate macro SET_GEOM_COORD_TIME_FUNCS without

@@ -58,6 +58,11 @@ CASES = [
     # connection by 4th-order differences every substep
     ("torus_dynmink_12x10x6_s1", "torus_dynmink", (12, 10, 6), 1, "load"),
     ("torus_dynmink_12x10x6_s3", "torus_dynmink", (12, 10, 6), 3, "load"),
+    # the circumbinary disk of the post-Newtonian binary setup
+    # (init.nz_pn_bbh_disk.c) on the same path, the Minkowski-spherical test
+    # spacetime standing in for the PN one the reference does not ship
+    ("pnbbh_dynmink_16x12x8_s1", "pnbbh_dynmink", (16, 12, 8), 1, "load"),
+    ("pnbbh_dynmink_16x12x8_s3", "pnbbh_dynmink", (16, 12, 8), 3, "load"),
 ]
 
 # Runs long enough for the flow to amplify a one-ulp change of pow() to O(1):

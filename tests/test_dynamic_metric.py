@@ -1,10 +1,12 @@
 """The time-dependent metric path (metric_dim 3; the reference's
 METRIC_GENERAL_DYNAMIC) against the reference's own build of it.
 
-Fixtures (tests/golden/make_golden.py, reference configuration
-torus_dynmink of oracle/build_ref.py): the magnetised torus setup on the
-dynamic path with the reference's Minkowski-spherical test spacetime,
-12x10x6 zones, 1 and 3 steps from the reference's own initial data.  The
+Fixtures (tests/golden/make_golden.py, reference configurations
+torus_dynmink and pnbbh_dynmink of oracle/build_ref.py): the magnetised
+torus setup (12x10x6 zones) and the post-Newtonian binary's circumbinary
+disk setup (16x12x8 zones, init.nz_pn_bbh_disk.c) on the dynamic path with
+the reference's Minkowski-spherical test spacetime, 1 and 3 steps from the
+reference's own initial data.  The
 reference keeps the geometry of three time levels in 3D tables (METRIC_DIM
 3), rotates them every step and rebuilds the connection before every
 substep by 4th-order differences of gcov (metric.c:3390-3690, conn.h).  The
@@ -30,6 +32,21 @@ import harmtest as ht
 NAMES = fixtures.dynamic_names()
 
 
+def metric_of(f):
+    """The configuration's COORD_DIAGONAL3 parameters and the driver's dt_conn."""
+    return hg.dyn_metric(**ht.CONFIG_DYN[str(f["config"])])
+
+
+def first_of_each_config():
+    seen, out = set(), []
+    for name in NAMES:
+        cfg = str(fixtures.load(name)["config"])
+        if cfg not in seen:
+            seen.add(cfg)
+            out.append(name)
+    return out
+
+
 def desc_of(f, precision=hg.PREC_FP64):
     sw = f["sw"]
     return hg.make_desc(f["n"], f["gam"], f["cour"], f["dx"], f["startx"], f["grid_length"], t=f["t0"],
@@ -47,12 +64,13 @@ def test_fixtures_are_the_dynamic_path():
         assert f["conn"].shape == (n[0] * n[1] * n[2], 64)
 
 
-def test_host_evaluation_matches_reference_tables():
-    f = fixtures.load(NAMES[0])
+@pytest.mark.parametrize("name", first_of_each_config())
+def test_host_evaluation_matches_reference_tables(name):
+    f = fixtures.load(name)
     n = f["n"]
     T = [x + 6 for x in n]
     d = desc_of(f)
-    m = hg.dyn_metric()
+    m = metric_of(f)
     ref = f["geom"]
     for pos in range(5):
         for i in range(T[0]):
@@ -77,7 +95,7 @@ def test_init_refuses_unsupported_dynamic_grids():
 
 def engine_for(f, precision=hg.PREC_FP64):
     e = hg.Engine(desc_of(f, precision))
-    e.set_dynamic_metric(hg.dyn_metric())
+    e.set_dynamic_metric(metric_of(f))
     e.set_cell_data(fixtures.cell6_of(f), f["rface"])
     e.set_cooling_tables(f["cool_omega"], f["cool_temp"])
     e.upload(f["p0"])
