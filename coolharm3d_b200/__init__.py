@@ -48,7 +48,8 @@ EXPORTS = ["hg_check_mirror", "hg_init", "hg_set_geometry", "hg_set_cell_data", 
            "hg_build_geometry_ks_mks", "hg_fixup_bounds", "hg_batch_create", "hg_batch_add", "hg_batch_remove",
            "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes",
            "hg_get_totals", "hg_get_launch_config", "hg_set_launch_config", "hg_autotune",
-           "hg_write_rdump", "hg_read_rdump", "hg_fp64_peak", "hg_set_dynamic_metric", "hg_dyn_geometry"]
+           "hg_write_rdump", "hg_read_rdump", "hg_fp64_peak", "hg_set_dynamic_metric", "hg_dyn_geometry",
+           "hg_dyn_geometry_block"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 DYN_MINK_SPHERICAL = 2
@@ -141,6 +142,8 @@ def load_library(path=LIB_PATH):
     lib.hg_set_dynamic_metric.argtypes = [P, P]
     lib.hg_dyn_geometry.argtypes = [ctypes.POINTER(GridDesc), P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                     ctypes.c_int32, ctypes.c_double, P]
+    lib.hg_dyn_geometry_block.argtypes = [ctypes.POINTER(GridDesc), P, ctypes.c_int32, ctypes.c_double,
+                                          ctypes.c_int32, ctypes.c_int32, P]
     lib.hg_get_totals.argtypes = [P, P, P, P]
     lib.hg_get_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
     lib.hg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
@@ -218,6 +221,16 @@ def ks_mks_tables(desc, a, R0=0.0, h_slope=0.35, th_cutout=1e-15 * np.pi, diag3_
                                         *[_ptr(out[k]) for k in ("geom", "conn", "cell6", "rface", "cool_omega",
                                                                  "cool_temp")]),
            "hg_build_geometry_ks_mks")
+    return out
+
+
+def dyn_geometry_block(desc, m, pos, t, i0, ni):
+    """hg_dyn_geometry_block: planes i0 .. i0+ni-1 of the struct of_geom the
+    device evaluates, (ni, N2TOT, N3TOT, 42), on the host."""
+    shp = ref_shape((desc.n1, desc.n2, desc.n3))
+    out = np.zeros((ni, shp[1], shp[2], NGEOM))
+    _check(load_library().hg_dyn_geometry_block(ctypes.byref(desc), ctypes.byref(m), pos, t, i0, ni, _ptr(out)),
+           "hg_dyn_geometry_block")
     return out
 
 

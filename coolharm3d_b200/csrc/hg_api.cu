@@ -845,6 +845,46 @@ extern "C" int hg_dyn_geometry(const hg_grid_desc *d, const hg_dyn_metric *m, in
   return HG_OK;
 }
 
+extern "C" int hg_dyn_geometry_block(const hg_grid_desc *d, const hg_dyn_metric *m, int32_t pos, double t,
+                                     int32_t i0, int32_t ni, double *geom)
+{
+  if (!d || !geom || pos < 0 || pos > 4 || ni < 0) return HG_ERR_BADARG;
+  const int T0 = d->n1 + 2 * HG_NGH, T1 = d->n2 + 2 * HG_NGH, T2 = d->n3 + 2 * HG_NGH;
+  if (i0 < 0 || i0 + ni > T0) return HG_ERR_BADARG;
+  GridDev G;
+  memset(&G, 0, sizeof(G));
+  int rc = dyn_from_abi(m, G.dyn);
+  if (rc != HG_OK) return rc;
+  for (int a = 0; a < 4; a++) {
+    G.startx[a] = d->startx[a];
+    G.dx[a] = d->dx[a];
+  }
+  const long rows = (long)ni * T1;
+  const int nw = (int)std::max<long>(1, std::min<long>(rows, std::max(1u, std::thread::hardware_concurrency())));
+  auto work = [&](int w) {
+    for (long r = w; r < rows; r += nw) {
+      const int i = i0 + (int)(r / T1), j = (int)(r % T1);
+      for (int k = 0; k < T2; k++) {
+        hg::Geom g;
+        hg::dyn_geom(G, pos, i, j, k, t, g);
+        double *o = geom + ((r * T2) + k) * HG_NGEOM;
+        memcpy(o, g.gcon, 16 * 8);
+        memcpy(o + 16, g.gcov, 16 * 8);
+        o[32] = g.g;
+        o[33] = g.g_inv;
+        o[34] = g.alpha;
+        for (int a = 0; a < 3; a++) o[35 + a] = g.beta[a];
+        for (int a = 0; a < 4; a++) o[38 + a] = g.ncon[a];
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int w = 1; w < nw; w++) th.emplace_back(work, w);
+  work(0);
+  for (auto &x : th) x.join();
+  return HG_OK;
+}
+
 extern "C" int hg_fixup_bounds(hg_handle *h)
 {
   if (!h) return HG_ERR_BADARG;

@@ -126,6 +126,14 @@ int hg_set_dynamic_metric(hg_handle *h, const hg_dyn_metric *m);
  * (exp, sincos, pow) are glibc's, the device's CUDA's. */
 int hg_dyn_geometry(const hg_grid_desc *desc, const hg_dyn_metric *m, int32_t pos, int32_t i, int32_t j, int32_t k,
                     double t, double geom[HG_NGEOM]);
+/* The same for whole planes i0 .. i0+ni-1 of the grid with ghost zones
+ * (every j, k of the reference layout), out[((i-i0)*N2TOT + j)*N3TOT + k]
+ * holding HG_NGEOM doubles; host threads.  For setups that turn a
+ * 4-velocity into primitives with the grid metric (init.*.c's ucon2pr) and
+ * take sqrt(-g) for their fields, as the reference's init_data() reads
+ * get_geometry() at t = 0.  No counterpart function in the reference. */
+int hg_dyn_geometry_block(const hg_grid_desc *desc, const hg_dyn_metric *m, int32_t pos, double t, int32_t i0,
+                          int32_t ni, double *geom);
 
 /* Primitive variables in the reference layout (flattened p[i][j][k][l]).
  * Upload is hg_upload_prims; download is what diag()/restart_write() need. */
