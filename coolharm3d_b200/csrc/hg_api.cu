@@ -430,8 +430,10 @@ extern "C" int hg_set_cell_data(hg_handle *h, const double *cell6, const double 
     if (!rface) return HG_ERR_BADARG;
     const int T0 = G.T[0];
     std::vector<double> r((size_t)12 * T0);
-    for (int i = 0; i < T0; i++) {  // rescale_prims_r(), recon.c:1142-1165
-      double rloc = cell6[(((long)i * N2T + HG_NGH) * N3T + HG_NGH) * 6 + 2];
+    // rescale_prims_r(), recon.c:1142-1165: x[RR] (the x1 column) of the
+    // zone centres of the row (i, N2S, N3S), as that row reads on its first call
+    for (int i = 0; i < T0; i++) {
+      double rloc = cell6[(((long)i * N2T + HG_NGH) * N3T + HG_NGH) * 6 + 3];
       double rf2 = rloc * rloc;
       r[0 * T0 + i] = sqrt(rf2 * rloc);
       r[1 * T0 + i] = rf2 * rloc;

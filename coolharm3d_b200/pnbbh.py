@@ -32,11 +32,12 @@ multiplicative lanes seeded from the C library's rand() after srand(seed).
 
 One side effect of the reference's setup carries into its run: init_prim()
 moves coords->x[RR] of every physical zone to the BL radius in place and
-moves it back only inside the disk (init.nz_pn_bbh_disk.c:494-507), and
-cooling_func_hr_disk() fills its tables later from x[RR] of the row
-(i, N2S, N3S) (phys.c:683-704).  That row lies outside the disk, so the
-reference cools with Omega and T of r + M there; cooling_tables() returns
-those tables.
+moves it back only inside the disk (init.nz_pn_bbh_disk.c:494-507), and both
+rescale_prims_r() and cooling_func_hr_disk() fill their tables on their
+first call from x[RR] of the row (i, N2S, N3S) (recon.c:1142-1165,
+phys.c:683-704).  That row lies outside the disk, so the reference's run
+scales and cools with r + M there.  driver_cell_data() gives the per-cell
+data with that column and cooling_tables() the tables from it.
 """
 import copy
 import ctypes
@@ -427,18 +428,29 @@ def _target_temperature(r, h_o_r, spin=SPIN):
     return 0.5 * math.pi * r_z * h_o_r * h_o_r * rm1
 
 
-def cooling_tables(desc, tables, inside, h_o_r=0.1):
-    """The cooling tables the reference's run uses after this setup: Omega and
-    T at x[RR] of (i, N2S, N3S), which init_prim() left at r + M for the
-    physical zones outside the disk (see the module docstring)."""
-    c6 = np.asarray(tables["cell6"])
+def driver_cell_data(desc, tables, inside):
+    """The per-cell data as the reference's driver holds it after this setup:
+    x1 (x[RR]) of the physical zones moved to r + M by init_prim(), and back
+    to (r + M) - M inside the disk.  RESCALE_R scales by this column
+    (hg_set_cell_data) and the cooling tables are evaluated on it."""
+    c6 = np.array(tables["cell6"], copy=True)
+    n1, n2, n3 = desc.n1, desc.n2, desc.n3
+    x = c6[NG:NG + n1, NG:NG + n2, NG:NG + n3, 3]
+    shifted = x + M_TOT
+    m = np.broadcast_to(inside[:, :, None], x.shape)
+    c6[NG:NG + n1, NG:NG + n2, NG:NG + n3, 3] = np.where(m, shifted - M_TOT, shifted)
+    return c6
+
+
+def cooling_tables(cell6, h_o_r=0.1):
+    """Omega and T of x[RR] along the row (i, N2S, N3S) of the driver's cell
+    data (driver_cell_data): the tables cooling_func_hr_disk() fills on its
+    first call (phys.c:683-704)."""
+    c6 = np.asarray(cell6)
     n1t = c6.shape[0]
     om, tt = np.empty(n1t), np.empty(n1t)
     for i in range(n1t):
         r = float(c6[i, NG, NG, 3])
-        ip = i - NG
-        if 0 <= ip < desc.n1 and not inside[ip, 0]:
-            r = r + M_TOT
         om[i] = _omega_circular(r)
         tt[i] = _target_temperature(r, h_o_r)
     return om, tt

@@ -90,7 +90,11 @@ int hg_set_geometry(hg_handle *h, const double *geom, int64_t n_geom, const doub
 
 /* Per-cell centre data in the reference layout, 6 doubles per cell:
  * rhoflr, uuflr, r, x1, x2, x3 (struct of_coord, coord.c:3754-3800);
- * rface[N1TOT]: x[RR] at FACE1 (RESCALE_R only, else NULL). */
+ * rface[N1TOT]: x[RR] at FACE1 (RESCALE_R only, else NULL).  RESCALE_R
+ * scales by x1 (x[RR]) of the row (i, N2S, N3S) and rface, the values
+ * rescale_prims_r() reads on its first call (recon.c:1142-1165): pass them
+ * as the driver holds them after its init (a setup that leaves x[RR] changed
+ * -- init.nz_pn_bbh_disk.c does -- changes the scaling the same way). */
 int hg_set_cell_data(hg_handle *h, const double *cell6, const double *rface);
 
 /* USE_COOLING_FUNCTION 1: per radial index i (N1TOT values each) the orbital

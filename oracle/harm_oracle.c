@@ -1741,7 +1741,7 @@ or_ctx *or_create(const or_desc *d, const double *geom, const double *conn, cons
   if (d->rescale_r) {
     for (int a = 0; a < 6; a++) c->rscale[a] = malloc(sizeof(double) * c->N1T);
     for (int i = 0; i < c->N1T; i++) { /* recon.c:1142-1165 */
-      double rloc = cell6[IX(c, i, NG, NG) * 6 + 2];
+      double rloc = cell6[IX(c, i, NG, NG) * 6 + 3]; /* x[RR] at CENT (recon.c:1146) */
       double rf2 = rloc * rloc;
       c->rscale[0][i] = sqrt(rf2 * rloc); c->rscale[1][i] = rf2 * rloc; c->rscale[2][i] = rloc;
       rloc = rface[i];

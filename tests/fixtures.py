@@ -44,6 +44,10 @@ def cell6_of(f):
     c = np.zeros(shape + (6,))
     c[..., :2] = f["cell_floors"]
     c[:, :, :, 2] = f["r_line"][:, None, None]
+    # x[RR] of the line (i, N2S, N3S), which RESCALE_R scales by; the same as
+    # r except where a setup left x[RR] changed (fixtures recorded before the
+    # column was kept have x[RR] = r)
+    c[:, :, :, 3] = f.get("x1_line", f["r_line"])[:, None, None]
     return c
 
 

@@ -146,9 +146,10 @@ def make(name, cfg, n, steps, seed):
         dx=geom["dx"], geom=geom["geom"], conn=geom["conn"],
         **{"sw_" + k: v for k, v in sw.items()})
     # floors at every cell centre (the engine's builder is checked against these),
-    # r along the line (i, N2S, N3S), r at FACE1 and the cooling tables per i
+    # r and x[RR] along the line (i, N2S, N3S), r at FACE1 and the cooling tables per i
     out["cell_floors"] = geom["cell6"][..., :2]
     out["r_line"] = geom["cell6"][:, ht.NG, ht.NG, 2]
+    out["x1_line"] = geom["cell6"][:, ht.NG, ht.NG, 3]
     out["rface"] = geom["rface"]
     out["cool_omega"] = geom["cool_omega"]
     out["cool_temp"] = geom["cool_temp"]

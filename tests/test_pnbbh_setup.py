@@ -63,13 +63,15 @@ def test_disk_matches_reference_initial_state_bit_for_bit():
         assert np.array_equal(p[..., l], f["p0"][..., l]), l
 
 
-def test_cooling_tables_are_the_reference_runs():
-    """Omega and T at r + M on the rows the setup's in-place BL shift left
-    behind, r elsewhere: exactly the tables the reference's run cools with."""
+def test_cell_data_and_cooling_tables_are_the_reference_runs():
+    """x[RR] at r + M where the setup's in-place BL shift was left behind, and
+    Omega, T from it: exactly what the reference's run scales and cools by."""
     f = fixtures.load(S1)
     n, d, t = grid(f)
     h = pnbbh.disk_fields(d, t, d.gam)
-    om, tt = pnbbh.cooling_tables(d, t, h["inside"])
+    c6 = pnbbh.driver_cell_data(d, t, h["inside"])
+    np.testing.assert_array_equal(c6[:, ht.NG, ht.NG, 3], f["x1_line"])
+    om, tt = pnbbh.cooling_tables(c6)
     np.testing.assert_array_equal(om, f["cool_omega"])
     np.testing.assert_array_equal(tt, f["cool_temp"])
     assert not np.array_equal(om, t["cool_omega"])   # the shift matters
@@ -103,9 +105,9 @@ def test_disk_on_engine_steps_like_the_reference():
     # zero): so does a fresh engine here
     e = hg.Engine(d)
     e.set_dynamic_metric(m)
-    e.set_cell_data(t["cell6"], t["rface"])
-    om, tt = pnbbh.cooling_tables(d, t, h["inside"])
-    e.set_cooling_tables(om, tt)
+    c6 = pnbbh.driver_cell_data(d, t, h["inside"])
+    e.set_cell_data(c6, t["rface"])
+    e.set_cooling_tables(*pnbbh.cooling_tables(c6))
     e.upload(p0)
     e.set_time(f3["t0"], f3["dt0"])
     e.step(f3["steps"])
