@@ -262,6 +262,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
       G.gS3 = (long)HG_NPOS * G.S;
       for (int l = 0; l < 3; l++) ALLOC(G.geomL[l], sizeof(double) * 42 * G.gS3);
       ALLOC(G.conn3, sizeof(double) * 64 * G.S);
+      ALLOC(G.ctab, sizeof(double) * hg::dyn_tab_layout(G.T).total);
     }
     if (G.rescale) ALLOC(G.rsc, sizeof(double) * 12 * G.T[0]);
     if (G.prec == HG_PREC_MIXED) {
@@ -815,6 +816,13 @@ extern "C" int hg_set_dynamic_metric(hg_handle *h, const hg_dyn_metric *m)
   int rc = dyn_from_abi(m, h->G.dyn);
   if (rc != HG_OK) return rc;
   HG_CK(cudaSetDevice(h->d.device));
+  {  // the coordinates' per-axis tables (the device reads, never evaluates, them)
+    GridDev Gh = h->G;
+    std::vector<double> tab((size_t)hg::dyn_tab_layout(Gh.T).total);
+    Gh.ctab = tab.data();
+    hg::dyn_coord_tables(Gh, tab.data());
+    HG_CK(copy_sync(h, h->G.ctab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+  }
   const int lev[3] = {0, 1, 2};  // n_beg, n_mid, n_end (init_general_metric, metric.c:3676-3679)
   HG_CK(copy_sync(h, sc_field(h->G, offsetof(hg::DevScalars, lev)), lev, sizeof(lev), cudaMemcpyHostToDevice));
   h->levels_stale = true;
@@ -835,6 +843,13 @@ extern "C" int hg_dyn_geometry(const hg_grid_desc *d, const hg_dyn_metric *m, in
     G.startx[a] = d->startx[a];
     G.dx[a] = d->dx[a];
   }
+  G.T[0] = d->n1 + 2 * HG_NGH;
+  G.T[1] = d->n2 + 2 * HG_NGH;
+  G.T[2] = d->n3 + 2 * HG_NGH;
+  if (i < 0 || j < 0 || k < 0 || i >= G.T[0] || j >= G.T[1] || k >= G.T[2]) return HG_ERR_BADARG;
+  std::vector<double> tab((size_t)hg::dyn_tab_layout(G.T).total);
+  hg::dyn_coord_tables(G, tab.data());
+  G.ctab = tab.data();
   hg::Geom g;
   hg::dyn_geom(G, pos, i, j, k, t, g);
   memcpy(geom, g.gcon, 16 * 8);
@@ -861,6 +876,12 @@ extern "C" int hg_dyn_geometry_block(const hg_grid_desc *d, const hg_dyn_metric 
     G.startx[a] = d->startx[a];
     G.dx[a] = d->dx[a];
   }
+  G.T[0] = T0;
+  G.T[1] = T1;
+  G.T[2] = T2;
+  std::vector<double> tab((size_t)hg::dyn_tab_layout(G.T).total);
+  hg::dyn_coord_tables(G, tab.data());
+  G.ctab = tab.data();
   const long rows = (long)ni * T1;
   const int nw = (int)std::max<long>(1, std::min<long>(rows, std::max(1u, std::thread::hardware_concurrency())));
   auto work = [&](int w) {
@@ -1309,7 +1330,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   b += sizeof(hg::DevScalars) + 8ull * cap * (2 + HG_NPR);  // scalars, queue, flagged list
   if (d->use_entropy_eq) b += 8ull * 6 * cap;                 // entropy face fluxes of the queue
   if (d->metric_dim == 2) b += 8ull * 42 * gS + 8ull * 64 * T[0] * T[1];
-  if (d->metric_dim == 3) b += 3ull * 8 * 42 * HG_NPOS * S + 8ull * 64 * S;
+  if (d->metric_dim == 3) b += 3ull * 8 * 42 * HG_NPOS * S + 8ull * 64 * S + 8ull * (4 * T[0] + 8 * T[1] + 4 * T[2]);  // coordinate tables
   if (d->rescale_r) b += 8ull * 12 * T[0];
   if (d->cooling) b += 8ull * 2 * T[0];
   if (d->precision == HG_PREC_MIXED) {

@@ -18,9 +18,12 @@
 // 468-472).  A post-Newtonian metric plugs in as one more gcov function.
 //
 // Every function restates the reference routine named beside it in the same
-// operation order; the elementary functions (exp, sincos, pow) are the
-// platform's, so the device's tables agree with the reference's to their
-// last-bit rounding, not bit for bit.
+// operation order.  The elementary functions of the coordinates (exp of x1,
+// the power of x2 and sincos of th; sincos of phi for spacetimes that need
+// Cartesian positions) depend on one index each: the host evaluates them with
+// the platform's libm into per-axis tables at faces and centres
+// (dyn_coord_tables), and the device and host evaluations read those, so the
+// device's geometry is the host's -- and the reference's -- bit for bit.
 #pragma once
 #include <math.h>
 
@@ -80,6 +83,27 @@ HG_DYN_HD void dyn_coords(const DynMetric &m, const double *xp, double *x, doubl
   *det = dx_dxp[0][0] * dx_dxp[3][3] * (dx_dxp[1][1] * dx_dxp[2][2] - dx_dxp[1][2] * dx_dxp[2][1]);
 }
 
+// Layout of GridDev::ctab (T = stored extents, every direction resolved):
+// per axis a value at 2*index + h, h = 0 at the face (index), 1 at the centre
+// (index + 1/2).
+struct DynTab {
+  int r, dr, th, dth, sth, cth, sph, cph, total;
+};
+HG_DYN_HD DynTab dyn_tab_layout(const int *T)
+{
+  DynTab L;
+  L.r = 0;
+  L.dr = L.r + 2 * T[0];
+  L.th = L.dr + 2 * T[0];
+  L.dth = L.th + 2 * T[1];
+  L.sth = L.dth + 2 * T[1];
+  L.cth = L.sth + 2 * T[1];
+  L.sph = L.cth + 2 * T[1];
+  L.cph = L.sph + 2 * T[2];
+  L.total = L.cph + 2 * T[2];
+  return L;
+}
+
 // trigvalues (metric.c:29-41): sincos with COORDSINGFIX
 HG_DYN_HD void dyn_trig(double th, double *cth, double *sth)
 {
@@ -132,41 +156,91 @@ HG_DYN_HD void dyn_gcon_sth(const double *x, double t2, double gcon[4][4])
 
 HG_DYN_HD double dyn_gdet_sth(const double *x, double t1) { return x[1] * x[1] * fabs(t1); }
 
+// The coordinates of a position from the tables: x (t, r, th, phi), the
+// diagonal Jacobian entries, sin/cos th, and dyn_coords' inverse and
+// determinant formed from them as dyn_coords forms them.
+struct DynPoint {
+  double x[4], a11, a22, i11, i22, det, sth, cth;
+};
+HG_DYN_HD void dyn_point(const GridDev &G, int pos, int i, int j, int k, double t, DynPoint &q)
+{
+  const DynTab L = dyn_tab_layout(G.T);
+  const double *c = G.ctab;
+  const int hi = (pos == 0 || pos == 4) ? 0 : 1, hj = (pos == 1 || pos == 4) ? 0 : 1;
+  const int ti = 2 * i + hi, tj = 2 * j + hj;
+  q.x[0] = t;
+  q.x[1] = c[L.r + ti];
+  q.x[2] = c[L.th + tj];
+  q.x[3] = G.startx[3] + (pos == 2 || pos == 4 ? (double)k : (k + 0.5)) * G.dx[3];
+  q.a11 = c[L.dr + ti];
+  q.a22 = c[L.dth + tj];
+  q.sth = c[L.sth + tj];
+  q.cth = c[L.cth + tj];
+  const double a12 = 0., a21 = 0.;
+  const double inv_det = 1. / (q.a11 * q.a22 - a12 * a21);
+  q.i11 = q.a22 * inv_det;
+  q.i22 = q.a11 * inv_det;
+  q.det = 1. * 1. * (q.a11 * q.a22 - a12 * a21);
+}
+
+// The tables on the host: r = R0 + exp(x1), th and the Jacobian by
+// dyn_coords, sin/cos th by trigvalues, sin/cos phi by sincos, at the face
+// and the centre of every index of each axis.
+inline void dyn_coord_tables(const GridDev &G, double *c)
+{
+  const DynTab L = dyn_tab_layout(G.T);
+  const int T0 = G.T[0], T1 = G.T[1], T2 = G.T[2];
+  for (int n = 0; n < 2 * (T0 > T1 ? (T0 > T2 ? T0 : T2) : (T1 > T2 ? T1 : T2)); n++) {
+    const double h = (n & 1) ? 0.5 : 0.;
+    const int idx = n >> 1;
+    double xp[4] = {0., G.startx[1] + (idx + h) * G.dx[1], G.startx[2] + (idx + h) * G.dx[2],
+                    G.startx[3] + (idx + h) * G.dx[3]};
+    double x[4], J[4][4], Ji[4][4], det;
+    dyn_coords(G.dyn, xp, x, J, Ji, &det);
+    if (idx < T0) {
+      c[L.r + n] = x[1];
+      c[L.dr + n] = J[1][1];
+    }
+    if (idx < T1) {
+      double cth, sth;
+      dyn_trig(x[2], &cth, &sth);
+      c[L.th + n] = x[2];
+      c[L.dth + n] = J[2][2];
+      c[L.sth + n] = sth;
+      c[L.cth + n] = cth;
+    }
+    if (idx < T2) {
+      double sp, cp;
+      sincos(x[3], &sp, &cp);
+      c[L.sph + n] = sp;
+      c[L.cph + n] = cp;
+    }
+  }
+}
+
 // The struct of_geom of one position at time t: set_general_geometry's loop
 // body (metric.c:3453-3483) with transform_all (coord.c:2340-2355:
 // transform_rank2cov2 / transform_rank2con2, coord.c:1852-1879, 1975-2002).
 HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t, Geom &g)
 {
-  const DynMetric &m = G.dyn;
-  double xp[4], x[4], dx_dxp[4][4], dxp_dx[4][4], det;
-  dyn_xp(G, pos, i, j, k, t, xp);
-  dyn_coords(m, xp, x, dx_dxp, dxp_dx, &det);
-  double gc[4][4], gn[4][4], cth, sth;
-  dyn_trig(x[2], &cth, &sth);
-  dyn_gcov_sth(x, sth, gc);
-  dyn_gcon_sth(x, sth, gn);
-  g.g = dyn_gdet_sth(x, sth);
+  DynPoint q;
+  dyn_point(G, pos, i, j, k, t, q);
+  double gc[4][4], gn[4][4];
+  dyn_gcov_sth(q.x, q.sth, gc);
+  dyn_gcon_sth(q.x, q.sth, gn);
+  g.g = dyn_gdet_sth(q.x, q.sth);
   // The sums of transform_rank2cov2/con2 in their order, leaving out the
   // terms whose Jacobian factor is exactly zero (most of them: COORD_DIAGONAL3
   // couples only r-x1 and th-x2); adding those zero products changes no sum.
+  const double J[4] = {1., q.a11, q.a22, 1.}, Ji[4] = {1., q.i11, q.i22, 1.};
 #pragma unroll
   for (int ip = 0; ip < 4; ip++)
 #pragma unroll
     for (int jp = 0; jp < 4; jp++) {
-      double c = 0., n = 0.;
-#pragma unroll
-      for (int a = 0; a < 4; a++) {
-        const double ja = dx_dxp[a][ip], ka = dxp_dx[ip][a];
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          if (ja != 0. && dx_dxp[b][jp] != 0.) c += gc[a][b] * ja * dx_dxp[b][jp];
-          if (ka != 0. && dxp_dx[jp][b] != 0.) n += gn[a][b] * ka * dxp_dx[jp][b];
-        }
-      }
-      g.gcov[ip][jp] = c;
-      g.gcon[ip][jp] = n;
+      g.gcov[ip][jp] = gc[ip][jp] * J[ip] * J[jp] + 0.;
+      g.gcon[ip][jp] = gn[ip][jp] * Ji[ip] * Ji[jp] + 0.;
     }
-  g.g *= det;
+  g.g *= q.det;
   g.g_inv = 1. / g.g;
   if (g.gcon[0][0] >= HG_GCON_EPS) g.gcon[0][0] = HG_GCON_EPS;
   g.ncon[0] = sqrt(-g.gcon[0][0]);
@@ -184,10 +258,9 @@ HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t
 // transform it here; it enters only the time derivative of the connection).
 HG_DYN_HD void dyn_gcov_func(const GridDev &G, int pos, int i, int j, int k, double t, double gcov[4][4])
 {
-  double xp[4], x[4], dx_dxp[4][4], dxp_dx[4][4], det;
-  dyn_xp(G, pos, i, j, k, t, xp);
-  dyn_coords(G.dyn, xp, x, dx_dxp, dxp_dx, &det);
-  dyn_gcov_x(G.dyn, x, gcov);
+  DynPoint q;
+  dyn_point(G, pos, i, j, k, t, q);
+  dyn_gcov_sth(q.x, q.sth, gcov);
 }
 
 }  // namespace hg

@@ -114,6 +114,10 @@ struct GridDev {
   long gS3;
   double *conn3;
   DynMetric dyn;
+  // metric_dim 3: per-axis coordinate tables at faces and centres (r, dr/dx1,
+  // th, dth/dx2, sin th, cos th, sin phi, cos phi), filled on the host with
+  // the platform's libm (dyn_coord_tables, hg_dyn.cuh)
+  double *ctab;
 };
 
 // Fixed grid sizes of the step's kernels (grid-stride loops).

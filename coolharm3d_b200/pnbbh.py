@@ -30,14 +30,12 @@ so they reproduce the reference's doubles; the grid-wide steps are numpy in
 the same order.  ranc() is restated from its algorithm (ranc.c): 64
 multiplicative lanes seeded from the C library's rand() after srand(seed).
 
-One side effect of the reference's setup carries into its run: init_prim()
-moves coords->x[RR] of every physical zone to the BL radius in place and
-moves it back only inside the disk (init.nz_pn_bbh_disk.c:494-507), and both
-rescale_prims_r() and cooling_func_hr_disk() fill their tables on their
-first call from x[RR] of the row (i, N2S, N3S) (recon.c:1142-1165,
-phys.c:683-704).  That row lies outside the disk, so the reference's run
-scales and cools with r + M there.  driver_cell_data() gives the per-cell
-data with that column and cooling_tables() the tables from it.
+The shipped setup moves the grid's stored coordinate x[RR] of every zone to
+the Boyer-Lindquist radius in place and moves it back only inside the disk
+(init.nz_pn_bbh_disk.c:494-507); the reference's run would then evaluate its
+metric, RESCALE_R and cooling tables at r + M outside the disk.  This setup
+leaves the grid's coordinates as they are (the reference configuration it
+is checked against restores them), so its tables are the grid's own.
 """
 import copy
 import ctypes
@@ -46,8 +44,8 @@ import math
 
 import numpy as np
 
-from . import (BC_SPHERICAL_OUTFLOW3, FLUX_HLLE, NG, PREC_FP64, RECON_PPM_MC, dyn_geometry, dyn_metric,
-               ks_mks_tables, make_desc, ref_shape)
+from . import (BC_SPHERICAL_OUTFLOW3, FLUX_HLLE, NG, PREC_FP64, RECON_PPM_MC, dyn_metric, ks_mks_tables, make_desc,
+               ref_shape)
 
 SMALL = 1.0e-15          # macros.h:441
 SINGSMALL = 1.0e-16      # options.h:271
@@ -405,55 +403,6 @@ def _bsq(pr, geo):
     bcon = [b0, (pr[5] + b0 * ucon[1]) * inv_ut, (pr[6] + b0 * ucon[2]) * inv_ut, (pr[7] + b0 * ucon[3]) * inv_ut]
     bcov = lower(bcon)
     return bcon[0] * bcov[0] + bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3]
-
-
-def _omega_circular(r, mass=M_TOT, spin=SPIN):
-    """omega_circular_equatorial (phys.c:861-905) with r_isco = 0, as the
-    setup sets it (init.nz_pn_bbh_disk.c:326)."""
-    return math.sqrt(mass) / (math.pow(r, 1.5) + spin)
-
-
-def _target_temperature(r, h_o_r, spin=SPIN):
-    """target_temperature (phys.c:805-848) outside r_isco = 0."""
-    rm1 = 1. / r
-    x = math.sqrt(r)
-    xm3 = 1. / (x * x * x)
-    term1 = spin * spin * rm1
-    c_f = 1. - 3 * rm1 + 2 * spin * xm3
-    f_f = 1. - 2 * spin * xm3 + term1 * rm1
-    g_f = 1. - 2 * rm1 + spin * xm3
-    ut_sq = g_f * g_f / c_f
-    uphi_sq = f_f * f_f * r / c_f
-    r_z = uphi_sq * rm1 - term1 * (ut_sq - 1.)
-    return 0.5 * math.pi * r_z * h_o_r * h_o_r * rm1
-
-
-def driver_cell_data(desc, tables, inside):
-    """The per-cell data as the reference's driver holds it after this setup:
-    x1 (x[RR]) of the physical zones moved to r + M by init_prim(), and back
-    to (r + M) - M inside the disk.  RESCALE_R scales by this column
-    (hg_set_cell_data) and the cooling tables are evaluated on it."""
-    c6 = np.array(tables["cell6"], copy=True)
-    n1, n2, n3 = desc.n1, desc.n2, desc.n3
-    x = c6[NG:NG + n1, NG:NG + n2, NG:NG + n3, 3]
-    shifted = x + M_TOT
-    m = np.broadcast_to(inside[:, :, None], x.shape)
-    c6[NG:NG + n1, NG:NG + n2, NG:NG + n3, 3] = np.where(m, shifted - M_TOT, shifted)
-    return c6
-
-
-def cooling_tables(cell6, h_o_r=0.1):
-    """Omega and T of x[RR] along the row (i, N2S, N3S) of the driver's cell
-    data (driver_cell_data): the tables cooling_func_hr_disk() fills on its
-    first call (phys.c:683-704)."""
-    c6 = np.asarray(cell6)
-    n1t = c6.shape[0]
-    om, tt = np.empty(n1t), np.empty(n1t)
-    for i in range(n1t):
-        r = float(c6[i, NG, NG, 3])
-        om[i] = _omega_circular(r)
-        tt[i] = _target_temperature(r, h_o_r)
-    return om, tt
 
 
 def set_disk(target, desc, tables, metric, beta=10.0, seed=1, t0=0.0, return_prims=True, plane_batch=16):

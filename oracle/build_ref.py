@@ -135,7 +135,16 @@ CONFIGS = {
     # size, the local prototype of init_prim() takes the struct of_coord * of
     # its definition, the diagnostic `rdiskout = x[RR]` reads coords->x[RR],
     # and get_rpmax()'s coords_loc is the struct of_coord that coord_of_r()
-    # fills (it was declared struct of_geom).
+    # fills (it was declared struct of_geom).  One behavioural fix: init_prim()
+    # moves the stored coordinate coords->x[RR] of each zone to the BL radius
+    # in place and moves it back only inside the disk (:494-507), so outside
+    # the disk the grid's coordinate arrays stay shifted by M; the reference's
+    # run then evaluates its metric there at r + M from the second step on
+    # (advance_geometry -> set_general_geometry reads get_coord,
+    # metric.c:398-430, 3390-3422) and builds its RESCALE_R and cooling
+    # tables from the shifted row (recon.c:1142-1165, phys.c:683-704).  The
+    # staged copy saves the coordinate and puts it back in both branches
+    # (exactly: (r + M) - M is not always r).
     "pnbbh_dynmink": ("init.nz_pn_bbh_disk.c",
                       dict(USE_COOLING_FUNCTION="(1)", FLUX_TYPE_CHOICE="(FLUX_HLLE)",
                            METRIC_TYPE_CHOICE="(METRIC_GENERAL_DYNAMIC)",
@@ -149,6 +158,12 @@ CONFIGS = {
                        ("Rout     = 100.*initial_bbh_separation;", "Rout     = 13.*initial_bbh_separation;"),
                        ("Rin = 0.05 * (initial_bbh_separation) ;", "Rin = 0.75 * (initial_bbh_separation) ;"),
                        ("beta     = 1.e2 ;", "beta     = 10. ;"),
+                       ("  coords->x[RR] += m_bh_tot;  /* Transform to BL coordinates */",
+                        "  const double x_rr_grid = coords->x[RR];\n  coords->x[RR] += m_bh_tot;"),
+                       ("    coords->x[RR] -= m_bh_tot;  /* Transform back from BL coordinates */",
+                        "    coords->x[RR] = x_rr_grid;"),
+                       ("  else { \n    PLOOP pr[l] = 0.;\n  }",
+                        "  else { \n    PLOOP pr[l] = 0.;\n    coords->x[RR] = x_rr_grid;\n  }"),
                        ("phys.c", "const double h_o_r  = 5.e-2;", "const double h_o_r  = 1.e-1;")]),
     # Advected field loop (Gardiner & Stone 2005), 2D periodic Minkowski:
     # PPM_MC + HLLE + para flux-CT, the shipped parameters.  The setup calls

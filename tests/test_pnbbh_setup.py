@@ -63,18 +63,14 @@ def test_disk_matches_reference_initial_state_bit_for_bit():
         assert np.array_equal(p[..., l], f["p0"][..., l]), l
 
 
-def test_cell_data_and_cooling_tables_are_the_reference_runs():
-    """x[RR] at r + M where the setup's in-place BL shift was left behind, and
-    Omega, T from it: exactly what the reference's run scales and cools by."""
+def test_cooling_tables_are_the_reference_runs():
+    """The cooling tables and the RESCALE_R row the reference's run uses are
+    the grid's own (the staged setup leaves the coordinates unshifted)."""
     f = fixtures.load(S1)
     n, d, t = grid(f)
-    h = pnbbh.disk_fields(d, t, d.gam)
-    c6 = pnbbh.driver_cell_data(d, t, h["inside"])
-    np.testing.assert_array_equal(c6[:, ht.NG, ht.NG, 3], f["x1_line"])
-    om, tt = pnbbh.cooling_tables(c6)
-    np.testing.assert_array_equal(om, f["cool_omega"])
-    np.testing.assert_array_equal(tt, f["cool_temp"])
-    assert not np.array_equal(om, t["cool_omega"])   # the shift matters
+    np.testing.assert_array_equal(t["cell6"][:, ht.NG, ht.NG, 3], f["x1_line"])
+    np.testing.assert_array_equal(t["cool_omega"], f["cool_omega"])
+    np.testing.assert_array_equal(t["cool_temp"], f["cool_temp"])
 
 
 def test_ranc_is_reseeded():
@@ -105,9 +101,8 @@ def test_disk_on_engine_steps_like_the_reference():
     # zero): so does a fresh engine here
     e = hg.Engine(d)
     e.set_dynamic_metric(m)
-    c6 = pnbbh.driver_cell_data(d, t, h["inside"])
-    e.set_cell_data(c6, t["rface"])
-    e.set_cooling_tables(*pnbbh.cooling_tables(c6))
+    e.set_cell_data(t["cell6"], t["rface"])
+    e.set_cooling_tables(t["cool_omega"], t["cool_temp"])
     e.upload(p0)
     e.set_time(f3["t0"], f3["dt0"])
     e.step(f3["steps"])
