@@ -15,12 +15,14 @@ engine evaluates the same geometry on the device (k_geom_level, k_conn_dyn).
   * On the host, the evaluation code (hg_dyn_geometry, compiled from the
     same source as the device kernels) reproduces the reference's tables
     bit for bit at all five positions of every zone.
-  * On the GPU the elementary functions of that code (exp, sincos, pow) are
-    CUDA's, which round differently from glibc's in the last bit, and the
-    entropy fix uses the correctly rounded pow (tests/test_crpow.py), so
-    the step is compared with a tolerance: primitives within 1e-12 of each
-    variable's largest magnitude after one step and 1e-10 after three, with
-    pflag and every failure counter exactly equal.
+  * On the GPU the coordinates' elementary functions come from per-axis
+    tables the host fills with the platform's libm, so the device's geometry
+    and connection are the reference's bit for bit; the entropy fix uses the
+    correctly rounded pow (tests/test_crpow.py), which moves a zone where
+    glibc's pow is misrounded by an ulp.  The bar: primitives within 1e-12 of
+    each variable's largest magnitude after one step and 1e-10 after three
+    (measured: 0, and 2e-25 in u on the disk), pflag and every failure
+    counter exactly equal.
 """
 import numpy as np
 import pytest
