@@ -49,23 +49,27 @@ EXPORTS = ["hg_check_mirror", "hg_init", "hg_set_geometry", "hg_set_cell_data", 
            "hg_batch_size", "hg_batch_step", "hg_batch_destroy", "hg_mem_info", "hg_grid_bytes",
            "hg_get_totals", "hg_get_launch_config", "hg_set_launch_config", "hg_autotune",
            "hg_write_rdump", "hg_read_rdump", "hg_fp64_peak", "hg_set_dynamic_metric", "hg_dyn_geometry",
-           "hg_dyn_geometry_block"]
+           "hg_dyn_geometry_block", "hg_download_dyn_level"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
 
 DYN_MINK_SPHERICAL = 2
+DYN_PN_BINARY = 3
 
 
 class DynMetric(ctypes.Structure):
     """hg_dyn_metric: the spacetime and COORD_DIAGONAL3 parameters of a
     metric_dim 3 (time-dependent metric) grid."""
     _fields_ = [("spacetime", ctypes.c_int32), ("diag3_exponent", ctypes.c_int32), ("R0", ctypes.c_double),
-                ("h_slope", ctypes.c_double), ("diag3_factor", ctypes.c_double), ("dt_conn", ctypes.c_double)]
+                ("h_slope", ctypes.c_double), ("diag3_factor", ctypes.c_double), ("dt_conn", ctypes.c_double),
+                ("m1", ctypes.c_double), ("m2", ctypes.c_double), ("separation", ctypes.c_double),
+                ("phase0", ctypes.c_double), ("inspiral", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
-def dyn_metric(spacetime=DYN_MINK_SPHERICAL, R0=0.0, h_slope=0.35, th_cutout=None, diag3_exponent=7, dt_conn=9.0e-6):
+def dyn_metric(spacetime=DYN_MINK_SPHERICAL, R0=0.0, h_slope=0.35, th_cutout=None, diag3_exponent=7, dt_conn=9.0e-6,
+               m1=0.5, m2=0.5, separation=20.0, phase0=0.0, inspiral=1):
     """The torus setup's coordinates (set_special_coord, init.torus.c:245-270:
-    th_cutout = SMALL pi, diag3_factor = 1 - 2 th_cutout/pi - h_slope) and the
-    driver's dt_conn (main.c:569)."""
+    th_cutout = SMALL pi, diag3_factor = 1 - 2 th_cutout/pi - h_slope), the
+    driver's dt_conn (main.c:569) and, for DYN_PN_BINARY, the binary."""
     import math
     if th_cutout is None:
         th_cutout = 1e-15 * math.pi
@@ -73,6 +77,7 @@ def dyn_metric(spacetime=DYN_MINK_SPHERICAL, R0=0.0, h_slope=0.35, th_cutout=Non
     m.spacetime, m.diag3_exponent, m.R0, m.h_slope = spacetime, diag3_exponent, R0, h_slope
     m.diag3_factor = 1. - 2 * th_cutout / math.pi - h_slope
     m.dt_conn = dt_conn
+    m.m1, m.m2, m.separation, m.phase0, m.inspiral = m1, m2, separation, phase0, inspiral
     return m
 
 
@@ -144,6 +149,7 @@ def load_library(path=LIB_PATH):
                                     ctypes.c_int32, ctypes.c_double, P]
     lib.hg_dyn_geometry_block.argtypes = [ctypes.POINTER(GridDesc), P, ctypes.c_int32, ctypes.c_double,
                                           ctypes.c_int32, ctypes.c_int32, P]
+    lib.hg_download_dyn_level.argtypes = [P, ctypes.c_int32, P]
     lib.hg_get_totals.argtypes = [P, P, P, P]
     lib.hg_get_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
     lib.hg_set_launch_config.argtypes = [P, ctypes.POINTER(LaunchConfig)]
@@ -295,6 +301,13 @@ class Engine:
             out = np.empty(self.shape + (NP,))
         assert out.shape == self.shape + (NP,) and out.dtype == np.float64 and out.flags.c_contiguous
         _check(self.lib.hg_download_prims(self.h, _ptr(out)), "hg_download_prims")
+        return out
+
+    def dyn_level(self, level=0):
+        """metric_dim 3: time level 0/1/2 (n_beg, n_mid, n_end) of the next
+        step as the device evaluated it, (5, N1TOT, N2TOT, N3TOT, 42)."""
+        out = np.empty((5,) + self.shape + (NGEOM,))
+        _check(self.lib.hg_download_dyn_level(self.h, level, _ptr(out)), "hg_download_dyn_level")
         return out
 
     def set_time(self, t, dt):

@@ -800,7 +800,17 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
 
 static int dyn_from_abi(const hg_dyn_metric *m, hg::DynMetric &dm)
 {
-  if (!m || m->spacetime != HG_DYN_MINK_SPHERICAL || m->diag3_exponent < 3 || !(m->dt_conn > 0.)) return HG_ERR_BADARG;
+  if (!m || (m->spacetime != HG_DYN_MINK_SPHERICAL && m->spacetime != HG_DYN_PN_BINARY) || m->diag3_exponent < 3 ||
+      !(m->dt_conn > 0.))
+    return HG_ERR_BADARG;
+  if (m->spacetime == HG_DYN_PN_BINARY &&
+      (!(m->m1 > 0.) || !(m->m2 > 0.) || !(m->separation > 0.) || (m->inspiral != 0 && m->inspiral != 1)))
+    return HG_ERR_BADARG;
+  dm.m1 = m->m1;
+  dm.m2 = m->m2;
+  dm.sep = m->separation;
+  dm.phase0 = m->phase0;
+  dm.inspiral = m->inspiral;
   dm.spacetime = m->spacetime;
   dm.diag3_exponent = m->diag3_exponent;
   dm.R0 = m->R0;
@@ -859,6 +869,30 @@ extern "C" int hg_dyn_geometry(const hg_grid_desc *d, const hg_dyn_metric *m, in
   geom[34] = g.alpha;
   for (int a = 0; a < 3; a++) geom[35 + a] = g.beta[a];
   for (int a = 0; a < 4; a++) geom[38 + a] = g.ncon[a];
+  return HG_OK;
+}
+
+extern "C" int hg_download_dyn_level(hg_handle *h, int32_t level, double *geom)
+{
+  if (!h || !geom || h->G.mdim != 3 || level < 0 || level > 2) return HG_ERR_BADARG;
+  if (!h->have_geom) return HG_ERR_STATE;
+  HG_CK(cudaSetDevice(h->d.device));
+  int rc = refresh_levels(h);
+  if (rc != HG_OK) return rc;
+  int lev[3];
+  HG_CK(copy_sync(h, lev, sc_field(h->G, offsetof(hg::DevScalars, lev)), sizeof(lev), cudaMemcpyDeviceToHost));
+  const GridDev &G = h->G;
+  std::vector<double> buf((size_t)42 * G.gS3);
+  HG_CK(copy_sync(h, buf.data(), G.geomL[lev[level]], sizeof(double) * buf.size(), cudaMemcpyDeviceToHost));
+  const long T0 = G.T[0], T1 = G.T[1], T2 = G.T[2];
+  for (int pos = 0; pos < HG_NPOS; pos++)
+    for (long i = 0; i < T0; i++)
+      for (long j = 0; j < T1; j++)
+        for (long k = 0; k < T2; k++) {
+          const long src = (long)pos * G.S + i * G.st[0] + j * G.st[1] + k * G.st[2];
+          double *o = geom + ((((long)pos * T0 + i) * T1 + j) * T2 + k) * HG_NGEOM;
+          for (int e = 0; e < HG_NGEOM; e++) o[e] = buf[(size_t)e * G.gS3 + src];
+        }
   return HG_OK;
 }
 

@@ -160,14 +160,15 @@ HG_DYN_HD double dyn_gdet_sth(const double *x, double t1) { return x[1] * x[1] *
 // diagonal Jacobian entries, sin/cos th, and dyn_coords' inverse and
 // determinant formed from them as dyn_coords forms them.
 struct DynPoint {
-  double x[4], a11, a22, i11, i22, det, sth, cth;
+  double x[4], a11, a22, i11, i22, det, sth, cth, sph, cph;
 };
 HG_DYN_HD void dyn_point(const GridDev &G, int pos, int i, int j, int k, double t, DynPoint &q)
 {
   const DynTab L = dyn_tab_layout(G.T);
   const double *c = G.ctab;
   const int hi = (pos == 0 || pos == 4) ? 0 : 1, hj = (pos == 1 || pos == 4) ? 0 : 1;
-  const int ti = 2 * i + hi, tj = 2 * j + hj;
+  const int hk = (pos == 2 || pos == 4) ? 0 : 1;
+  const int ti = 2 * i + hi, tj = 2 * j + hj, tk = 2 * k + hk;
   q.x[0] = t;
   q.x[1] = c[L.r + ti];
   q.x[2] = c[L.th + tj];
@@ -176,6 +177,8 @@ HG_DYN_HD void dyn_point(const GridDev &G, int pos, int i, int j, int k, double 
   q.a22 = c[L.dth + tj];
   q.sth = c[L.sth + tj];
   q.cth = c[L.cth + tj];
+  q.sph = c[L.sph + tk];
+  q.cph = c[L.cph + tk];
   const double a12 = 0., a21 = 0.;
   const double inv_det = 1. / (q.a11 * q.a22 - a12 * a21);
   q.i11 = q.a22 * inv_det;
@@ -218,6 +221,109 @@ inline void dyn_coord_tables(const GridDev &G, double *c)
   }
 }
 
+// ---------------------------------------------------------------------------
+// HG_DYN_PN_BINARY: the binary's positions and velocities at time t, and the
+// first post-Newtonian harmonic-gauge metric of two point masses
+//   g00 = -1 + 2V - 2V^2,  g0i = -4 V_i,  gij = (1 + 2V) delta_ij,
+//   V = sum m_a / r_a,  V_i = sum m_a v_a^i / r_a
+// (the 1PN metric written with the potentials V, V_i, e.g. Blanchet, Faye &
+// Ponsot 1998, Phys. Rev. D 58 124002, eq. 7.2 at this order, with V and V_i
+// at their instantaneous point-mass values).  No counterpart in the
+// reference's sources, whose PN metric bodies are absent.
+struct PNBinary {
+  double y[2][3], v[2][3], m[2];
+};
+
+// Quasi-circular orbit: the separation shrinks by the quadrupole formula
+// (Peters 1964): r^4 = r0^4 - (256/5) eta M^3 t, dr/dt = -(64/5) eta M^3 / r^3,
+// phase phi0 + (r0^(5/2) - r^(5/2)) / (32 eta M^(5/2)) (the integral of
+// Omega = sqrt(M / r^3)); without inspiral r = r0, phi = phi0 + Omega t.
+// m1 sits at +m2/M r n, m2 at -m1/M r n, n = (cos phi, sin phi, 0).
+HG_DYN_HD void pn_binary(const DynMetric &dm, double t, PNBinary &b)
+{
+  const double M = dm.m1 + dm.m2, eta = dm.m1 * dm.m2 / (M * M);
+  const double r0 = dm.sep, M3 = M * M * M;
+  double r = r0, rdot = 0., phi;
+  if (dm.inspiral) {
+    double q = r0 * r0 * r0 * r0 - (256. / 5.) * eta * M3 * t;
+    const double qmin = 1.e-12 * r0 * r0 * r0 * r0;  // past coalescence: hold the smallest orbit
+    if (q < qmin) q = qmin;
+    r = sqrt(sqrt(q));
+    rdot = -(64. / 5.) * eta * M3 / (r * r * r);
+    phi = dm.phase0 + (r0 * r0 * sqrt(r0) - r * r * sqrt(r)) / (32. * eta * M * M * sqrt(M));
+  } else {
+    phi = dm.phase0 + sqrt(M / (r * r * r)) * t;
+  }
+  const double om = sqrt(M / (r * r * r));
+  double sp, cp;
+  sincos(phi, &sp, &cp);
+  const double f[2] = {dm.m2 / M, -dm.m1 / M};
+  b.m[0] = dm.m1;
+  b.m[1] = dm.m2;
+  for (int a = 0; a < 2; a++) {
+    b.y[a][0] = f[a] * r * cp;
+    b.y[a][1] = f[a] * r * sp;
+    b.y[a][2] = 0.;
+    b.v[a][0] = f[a] * (rdot * cp - r * om * sp);
+    b.v[a][1] = f[a] * (rdot * sp + r * om * cp);
+    b.v[a][2] = 0.;
+  }
+}
+
+// gcov, gcon and sqrt(-g) of the PN metric at a position, in the grid's
+// numerical coordinates: gcov = J^T g_cart J with J = d(t,x,y,z)/d(t,x1,x2,x3)
+// (Cartesian of the spherical r, th, phi of the COORD_DIAGONAL3 point), gcon
+// = K g_cart^-1 K^T with K = J^-1, and g_cart^-1 from the block form of
+// g_cart: with A = 1 + 2V, w = g0i and s = g00 - w.w / A,
+// g^00 = 1/s, g^0i = -w_i / (A s), g^ij = delta_ij / A + w_i w_j / (A^2 s),
+// det g_cart = A^3 s.
+HG_DYN_HD void pn_metric(const DynMetric &dm, const DynPoint &q, double gcov[4][4], double gcon[4][4],
+                         double *gdet)
+{
+  PNBinary b;
+  pn_binary(dm, q.x[0], b);
+  const double r = q.x[1];
+  const double X[3] = {r * q.sth * q.cph, r * q.sth * q.sph, r * q.cth};
+  double V = 0., Vi[3] = {0., 0., 0.};
+  for (int a = 0; a < 2; a++) {
+    const double d0 = X[0] - b.y[a][0], d1 = X[1] - b.y[a][1], d2 = X[2] - b.y[a][2];
+    const double ra = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    const double ma = b.m[a] / ra;
+    V += ma;
+    for (int c = 0; c < 3; c++) Vi[c] += ma * b.v[a][c];
+  }
+  const double A = 1. + 2. * V;
+  const double g00 = -1. + 2. * V - 2. * V * V;
+  const double w[3] = {-4. * Vi[0], -4. * Vi[1], -4. * Vi[2]};
+  // columns of J (x1, x2, x3) and rows of K = J^-1
+  const double J[3][3] = {{q.a11 * q.sth * q.cph, q.a11 * q.sth * q.sph, q.a11 * q.cth},
+                          {q.a22 * r * q.cth * q.cph, q.a22 * r * q.cth * q.sph, -q.a22 * r * q.sth},
+                          {-r * q.sth * q.sph, r * q.sth * q.cph, 0.}};
+  const double ir = 1. / r, irs = 1. / (r * q.sth);
+  const double K[3][3] = {{q.i11 * q.sth * q.cph, q.i11 * q.sth * q.sph, q.i11 * q.cth},
+                          {q.i22 * ir * q.cth * q.cph, q.i22 * ir * q.cth * q.sph, -q.i22 * ir * q.sth},
+                          {-irs * q.sph, irs * q.cph, 0.}};
+  gcov[0][0] = g00;
+  for (int a = 0; a < 3; a++) {
+    const double c = w[0] * J[a][0] + w[1] * J[a][1] + w[2] * J[a][2];
+    gcov[0][a + 1] = c;
+    gcov[a + 1][0] = c;
+    for (int e = 0; e < 3; e++) gcov[a + 1][e + 1] = A * (J[a][0] * J[e][0] + J[a][1] * J[e][1] + J[a][2] * J[e][2]);
+  }
+  const double s = g00 - (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]) / A;
+  const double iAs = 1. / (A * s);
+  double Kw[3];
+  for (int a = 0; a < 3; a++) Kw[a] = K[a][0] * w[0] + K[a][1] * w[1] + K[a][2] * w[2];
+  gcon[0][0] = 1. / s;
+  for (int a = 0; a < 3; a++) {
+    gcon[0][a + 1] = -Kw[a] * iAs;
+    gcon[a + 1][0] = gcon[0][a + 1];
+    for (int e = 0; e < 3; e++)
+      gcon[a + 1][e + 1] = (K[a][0] * K[e][0] + K[a][1] * K[e][1] + K[a][2] * K[e][2]) / A + Kw[a] * Kw[e] * iAs / A;
+  }
+  *gdet = sqrt(-(A * A * A * s)) * fabs(q.det * r * r * q.sth);
+}
+
 // The struct of_geom of one position at time t: set_general_geometry's loop
 // body (metric.c:3453-3483) with transform_all (coord.c:2340-2355:
 // transform_rank2cov2 / transform_rank2con2, coord.c:1852-1879, 1975-2002).
@@ -225,6 +331,9 @@ HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t
 {
   DynPoint q;
   dyn_point(G, pos, i, j, k, t, q);
+  if (G.dyn.spacetime == HG_DYN_PN_BINARY) {
+    pn_metric(G.dyn, q, g.gcov, g.gcon, &g.g);
+  } else {
   double gc[4][4], gn[4][4];
   dyn_gcov_sth(q.x, q.sth, gc);
   dyn_gcon_sth(q.x, q.sth, gn);
@@ -241,6 +350,7 @@ HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t
       g.gcon[ip][jp] = gn[ip][jp] * Ji[ip] * Ji[jp] + 0.;
     }
   g.g *= q.det;
+  }
   g.g_inv = 1. / g.g;
   if (g.gcon[0][0] >= HG_GCON_EPS) g.gcon[0][0] = HG_GCON_EPS;
   g.ncon[0] = sqrt(-g.gcon[0][0]);
@@ -254,13 +364,20 @@ HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t
 }
 
 // gcov_func() of the dynamic path (metric.c:3943-3981): the spacetime's
-// metric at a position, in its own coordinates (the reference does not
-// transform it here; it enters only the time derivative of the connection).
+// metric at a position, for the time derivative of the connection.  A
+// spacetime in the grid's own (spherical) topology is not transformed there;
+// a Cartesian one -- the PN binary -- is taken to the numerical coordinates
+// (transform_rank2cov2 with dxc_dxp, metric.c:3968-3976).
 HG_DYN_HD void dyn_gcov_func(const GridDev &G, int pos, int i, int j, int k, double t, double gcov[4][4])
 {
   DynPoint q;
   dyn_point(G, pos, i, j, k, t, q);
-  dyn_gcov_sth(q.x, q.sth, gcov);
+  if (G.dyn.spacetime == HG_DYN_PN_BINARY) {
+    double gcon[4][4], gdet;
+    pn_metric(G.dyn, q, gcov, gcon, &gdet);
+  } else {
+    dyn_gcov_sth(q.x, q.sth, gcov);
+  }
 }
 
 }  // namespace hg

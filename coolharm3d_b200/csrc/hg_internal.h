@@ -50,6 +50,8 @@ struct DynMetric {
   int diag3_exponent;
   double R0, h_slope, diag3_factor;
   double dt_conn;      // half-width of the connection's time difference (main.c:569)
+  double m1, m2, sep, phase0;  // HG_DYN_PN_BINARY: the binary
+  int inspiral;
 };
 
 // Device-resident scalars of one grid (t, dx[0], reductions, failure flags).

@@ -405,6 +405,38 @@ def _bsq(pr, geo):
     return bcon[0] * bcov[0] + bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3]
 
 
+def _omega_circular(r, mass=M_TOT, spin=SPIN):
+    """omega_circular_equatorial (phys.c:861-905) with r_isco = 0 (the
+    setup's, init.nz_pn_bbh_disk.c:326)."""
+    return math.sqrt(mass) / (math.pow(r, 1.5) + spin)
+
+
+def _target_temperature(r, h_o_r, spin=SPIN):
+    """target_temperature (phys.c:805-848) outside r_isco = 0."""
+    rm1 = 1. / r
+    x = math.sqrt(r)
+    xm3 = 1. / (x * x * x)
+    term1 = spin * spin * rm1
+    c_f = 1. - 3 * rm1 + 2 * spin * xm3
+    f_f = 1. - 2 * spin * xm3 + term1 * rm1
+    g_f = 1. - 2 * rm1 + spin * xm3
+    ut_sq = g_f * g_f / c_f
+    uphi_sq = f_f * f_f * r / c_f
+    r_z = uphi_sq * rm1 - term1 * (ut_sq - 1.)
+    return 0.5 * math.pi * r_z * h_o_r * h_o_r * rm1
+
+
+def pn_cooling_tables(tables, h_o_r=0.1):
+    """Cooling tables of a run in a post-Newtonian (harmonic-coordinate)
+    metric: the reference takes Omega and T at the Boyer-Lindquist radius
+    r + M there (USE_ISOTROPIC_COORDS, phys.c:829-831, 888-891), along the
+    row (i, N2S, N3S) it tabulates (phys.c:683-704)."""
+    c6 = np.asarray(tables["cell6"])
+    om = np.array([_omega_circular(float(r) + M_TOT) for r in c6[:, NG, NG, 3]])
+    tt = np.array([_target_temperature(float(r) + M_TOT, h_o_r) for r in c6[:, NG, NG, 3]])
+    return om, tt
+
+
 def set_disk(target, desc, tables, metric, beta=10.0, seed=1, t0=0.0, return_prims=True, plane_batch=16):
     """Initial data of the circumbinary disk on `target` (init_data,
     init.nz_pn_bbh_disk.c:216-300) for the grid metric `metric` (an

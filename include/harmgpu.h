@@ -113,14 +113,31 @@ int hg_set_cooling_tables(hg_handle *h, const double *omega, const double *t_tar
  * metric.c:3507-3648, conn.h).  The spacetime and its COORD_DIAGONAL3
  * coordinates (coord.c:270-276, set_special_coord of the setup) are
  * described here.  Spacetimes: HG_DYN_MINK_SPHERICAL, the reference's
- * METRIC_DYNAMIC_MINK_SPHERICAL test spacetime (options.h:90).  Every
- * direction must be resolved (N > 1); FP64 forms only. */
+ * METRIC_DYNAMIC_MINK_SPHERICAL test spacetime (options.h:90), and
+ * HG_DYN_PN_BINARY below.  Every direction must be resolved (N > 1); FP64
+ * forms only. */
 #define HG_DYN_MINK_SPHERICAL 2
+/* HG_DYN_PN_BINARY: two point masses m1, m2 on a quasi-circular orbit in the
+ * equatorial plane, in the first post-Newtonian harmonic-gauge metric
+ *   g00 = -1 + 2V - 2V^2,  g0i = -4 V_i,  gij = (1 + 2V) delta_ij,
+ * V = m1/r1 + m2/r2, V_i = m1 v1^i/r1 + m2 v2^i/r2 (the potentials at their
+ * instantaneous point-mass values), taken to the grid's spherical
+ * COORD_DIAGONAL3 coordinates; the separation shrinks by the quadrupole
+ * formula when inspiral is 1 (Peters 1964), else the orbit is a circle.
+ * The reference's own PN metrics (METRIC_DYNAMIC_FULLPN_*, metric.h:105-171)
+ * have no bodies in its sources: this spacetime has no counterpart there. */
+#define HG_DYN_PN_BINARY 3
 typedef struct hg_dyn_metric {
   int32_t spacetime;            /* HG_DYN_* */
   int32_t diag3_exponent;       /* COORD_DIAGONAL3: odd, >= 3 */
   double R0, h_slope, diag3_factor;
   double dt_conn;               /* main.c:569 sets 9e-6 */
+  /* HG_DYN_PN_BINARY only */
+  double m1, m2;                /* masses, m1 on the +x axis at t = 0 when phase0 = 0 */
+  double separation;            /* separation at t = 0 (harmonic coordinates) */
+  double phase0;                /* orbital phase at t = 0 */
+  int32_t inspiral;             /* 1: quadrupole-formula inspiral; 0: circular orbit */
+  int32_t reserved;
 } hg_dyn_metric;
 int hg_set_dynamic_metric(hg_handle *h, const hg_dyn_metric *m);
 /* The struct of_geom (HG_NGEOM doubles, hg_set_geometry's order) of position
@@ -138,6 +155,11 @@ int hg_dyn_geometry(const hg_grid_desc *desc, const hg_dyn_metric *m, int32_t po
  * get_geometry() at t = 0.  No counterpart function in the reference. */
 int hg_dyn_geometry_block(const hg_grid_desc *desc, const hg_dyn_metric *m, int32_t pos, double t, int32_t i0,
                           int32_t ni, double *geom);
+/* metric_dim 3: the time level `level` (0 n_beg, 1 n_mid, 2 n_end) of the
+ * step about to run, as the device evaluated it, in the reference's layout
+ * out[(((pos*N1TOT + i)*N2TOT + j)*N3TOT + k)*HG_NGEOM + e] (the geom_arr of
+ * METRIC_DIM 3, decomp.c:168): for checking the device's evaluation. */
+int hg_download_dyn_level(hg_handle *h, int32_t level, double *geom);
 
 /* Primitive variables in the reference layout (flattened p[i][j][k][l]).
  * Upload is hg_upload_prims; download is what diag()/restart_write() need. */

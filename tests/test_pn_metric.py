@@ -1,0 +1,174 @@
+"""The post-Newtonian binary spacetime of the dynamic-metric path
+(HG_DYN_PN_BINARY): two point masses on a quasi-circular orbit in the first
+post-Newtonian harmonic-gauge metric, evaluated in the kernels at every time
+level and in the connection's time derivative every substep.
+
+The reference's own PN metric bodies are absent from its sources, so this
+spacetime is parity unpinned: it is checked by its properties (inverse and
+determinant, the equal-mass pi symmetry, stationarity of the circular orbit
+in the co-rotating frame, the Newtonian potential, the far field), and the
+device's evaluation against the host's.  The circumbinary disk of the
+post-Newtonian binary setup then runs in it."""
+import math
+
+import numpy as np
+import pytest
+
+import coolharm3d_b200 as hg
+import harmtest as ht
+from coolharm3d_b200 import pnbbh
+
+N = (16, 12, 8)
+
+
+def geom(d, m, pos, i, j, k, t=0.0):
+    g = hg.dyn_geometry(d, m, pos, i, j, k, t)
+    return g[16:32].reshape(4, 4), g[0:16].reshape(4, 4), g[32]
+
+
+def pn(**kw):
+    return pnbbh.pnbbh_coords(spacetime=hg.DYN_PN_BINARY, **kw)
+
+
+def test_inverse_and_determinant():
+    d = pnbbh.pnbbh_desc(N)
+    for m in (pn(inspiral=0), pn(inspiral=1, phase0=0.3)):
+        for pos in range(5):
+            for (i, j, k) in [(3, 3, 3), (5, 7, 2), (18, 10, 9), (10, 8, 5), (0, 0, 0), (21, 17, 13)]:
+                gc, gn, gd = geom(d, m, pos, i, j, k, 7.0)
+                assert np.abs(gc @ gn - np.eye(4)).max() < 1e-13
+                assert abs(math.sqrt(-np.linalg.det(gc)) - gd) < 1e-13 * gd
+                assert np.array_equal(gc, gc.T) and np.array_equal(gn, gn.T)
+
+
+def test_equal_masses_are_symmetric_under_half_turn():
+    d = pnbbh.pnbbh_desc(N)     # 8 zones in phi: k + 4 is phi + pi
+    m = pn(inspiral=1)
+    for (i, j, k) in [(3, 3, 3), (10, 8, 4), (15, 5, 6)]:
+        a = geom(d, m, 3, i, j, k, 11.0)[0]
+        b = geom(d, m, 3, i, j, k + 4, 11.0)[0]
+        assert np.abs(a - b).max() <= 1e-15 * np.abs(a).max()
+
+
+def test_circular_orbit_is_stationary_when_co_rotating():
+    d = pnbbh.pnbbh_desc(N)
+    m = pn(inspiral=0)
+    om = math.sqrt(1.0 / 20.0 ** 3)
+    dphi = 2 * math.pi / N[2]
+    for (i, j) in [(9, 6), (4, 9)]:
+        a = geom(d, m, 3, i, j, 3, 0.0)[0]
+        b = geom(d, m, 3, i, j, 4, dphi / om)[0]
+        assert np.abs(a - b).max() <= 1e-14 * np.abs(a).max()
+
+
+def test_inspiral_shrinks_the_orbit_and_the_potential_follows():
+    """g_tt at a point follows -1 + 2V - 2V^2 of the masses at the Peters
+    separation r(t)^4 = r0^4 - (256/5) eta M^3 t."""
+    d = pnbbh.pnbbh_desc(N)
+    m = pn(inspiral=1)
+    t = 1.0e4          # coalescence at r0^4 / ((256/5) eta M^3) = 12500
+    r12 = (20.0 ** 4 - 256.0 / 5.0 * 0.25 * t) ** 0.25
+    phase = (20.0 ** 2.5 - r12 ** 2.5) / (32 * 0.25)
+    c6 = pnbbh.pnbbh_tables(d)["cell6"]
+    for (i, j, k) in [(3, 7, 3), (8, 6, 5)]:
+        r, th = c6[i, j, k, 3], c6[i, j, k, 4]
+        ph = d.startx[3] + (k + 0.5) * d.dx[3]
+        X = np.array([r * math.sin(th) * math.cos(ph), r * math.sin(th) * math.sin(ph), r * math.cos(th)])
+        y = 0.5 * r12 * np.array([math.cos(phase), math.sin(phase), 0.0])
+        V = 0.5 / np.linalg.norm(X - y) + 0.5 / np.linalg.norm(X + y)
+        assert geom(d, m, 3, i, j, k, t)[0][0, 0] == pytest.approx(-1 + 2 * V - 2 * V * V, rel=1e-13)
+
+
+def test_far_field_is_flat():
+    """At the grid's outer radius the metric differs from the flat one by the
+    monopole 2M/r."""
+    d = pnbbh.pnbbh_desc(N)
+    i = N[0] + 2
+    gp = geom(d, pn(), 3, i, 6, 3)[0]
+    gm = geom(d, pnbbh.pnbbh_coords(), 3, i, 6, 3)[0]
+    r = pnbbh.pnbbh_tables(d)["cell6"][i, 6, 3, 3]
+    assert gp[0, 0] + 1.0 == pytest.approx(2.0 / r, rel=0.02)
+    assert np.abs(gp - gm).max() <= 3.0 / r * np.abs(gm).max()
+
+
+def test_bad_binaries_are_refused():
+    d = pnbbh.pnbbh_desc(N)
+    out = np.zeros(hg.NGEOM)
+    lib = hg.load_library()
+    import ctypes
+    for kw in (dict(m1=0.0), dict(m2=-1.0), dict(separation=0.0), dict(inspiral=2)):
+        m = pn(**kw)
+        rc = lib.hg_dyn_geometry(ctypes.byref(d), ctypes.byref(m), 3, 4, 4, 4, 0.0,
+                                 out.ctypes.data_as(ctypes.c_void_p))
+        assert rc == -2, kw   # HG_ERR_BADARG
+
+
+def engine(m, n=N):
+    d = pnbbh.pnbbh_desc(n)
+    t = pnbbh.pnbbh_tables(d)
+    e = hg.Engine(d)
+    e.set_dynamic_metric(m)
+    e.set_cell_data(t["cell6"], t["rface"])
+    return e, d, t
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spacetime", ["mink", "pn"])
+def test_device_levels_match_host(spacetime):
+    """The three time levels the device evaluated against the host's
+    evaluation at t0, t0 + dt/2, t0 + dt: bit for bit for the Minkowski
+    stand-in (table-driven coordinates); for the PN binary within rounding
+    (the orbit's sincos and sqrt are the device's)."""
+    m = pnbbh.pnbbh_coords() if spacetime == "mink" else pn(inspiral=1, phase0=0.4)
+    e, d, t = engine(m)
+    t0, dt = 3.0, 1.0e-2
+    e.upload(np.zeros(e.shape + (8,)))
+    e.set_time(t0, dt)
+    for lev, tl in ((0, t0), (1, t0 + 0.5 * dt), (2, t0 + dt)):
+        dev = e.dyn_level(lev)
+        host = np.stack([hg.dyn_geometry_block(d, m, pos, tl, 0, e.shape[0]) for pos in range(5)])
+        if spacetime == "mink":
+            assert np.array_equal(dev, host), lev
+        else:
+            scale = np.abs(host).reshape(-1, 42).max(0)
+            err = (np.abs(dev - host).reshape(-1, 42).max(0) / np.where(scale > 0, scale, 1.0)).max()
+            assert err < 1e-13, (lev, err)
+    e.close()
+
+
+@pytest.mark.gpu
+def test_disk_runs_in_the_pn_metric():
+    """The circumbinary disk set up in the PN metric and stepped: the state
+    stays finite, the PN metric changes the flow (against the Minkowski
+    stand-in from the same start), and steps in one call equal steps one by
+    one (the time levels rotate on the device)."""
+    m = pn(inspiral=1)
+    e, d, t = engine(m)
+    p0, h = pnbbh.set_disk(e, d, t, m)
+    om, tt = pnbbh.pn_cooling_tables(t)
+    e.set_cooling_tables(om, tt)
+    e.close()
+
+    def run(metric, nsteps, one_by_one=False):
+        e, _, _ = engine(metric)
+        e.set_cooling_tables(om, tt)
+        e.upload(p0)
+        e.set_time(0.0, d.dx[0])
+        if one_by_one:
+            for _ in range(nsteps):
+                e.step(1)
+        else:
+            e.step(nsteps)
+        out = (e.download(), e.fail_counts())
+        e.close()
+        return out
+
+    p, fc = run(m, 6)
+    assert np.isfinite(p).all()
+    assert np.array_equal(p, run(m, 6, one_by_one=True)[0])
+    pm, _ = run(pnbbh.pnbbh_coords(), 6)
+    inside = np.broadcast_to(h["inside"][:, :, None], (N[0], N[1], N[2]))
+    a, b = ht.interior(p, N), ht.interior(pm, N)
+    # the radial velocity the flow develops differs by far more than rounding
+    # (measured: 1e-4 of itself after six steps, t ~ 1e-4)
+    assert np.abs(a[inside][:, 2] - b[inside][:, 2]).max() > 1e-6 * np.abs(b[inside][:, 2]).max()
