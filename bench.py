@@ -70,6 +70,12 @@ def parse():
     return ap.parse_args()
 
 
+# the reference has no PN metric bodies: its arm for the binary-disk
+# workloads runs the same setup on its dynamic path with the Minkowski test
+# spacetime (geometry of the time levels and the connection rebuilt the same
+# way, a cheaper metric function)
+PN_REF_NOTE = "; the reference's Minkowski-spherical test spacetime in place of the PN metric it does not ship"
+
 WORKLOADS = {
     "torus192": dict(kind="torus", n=(192, 192, 128), ref_cfg="torus",
                      label="Fishbone-Moncrief torus, Kerr-Schild a=0.9, MKS 192x192x128, r_in 6, r_pmax 12, "
@@ -82,6 +88,14 @@ WORKLOADS = {
                         label="torus192's initial state on the time-dependent metric path (metric_dim 3): the "
                               "Minkowski-spherical test spacetime, geometry of three time levels and the "
                               "finite-difference connection evaluated on the device every step, FP64"),
+    "pnbbh300": dict(kind="pnbbh", n=(300, 160, 400), ref_cfg="pnbbh_dynmink", ref_note=PN_REF_NOTE,
+                     label="circumbinary disk of an equal-mass black-hole binary (the post-Newtonian binary disk "
+                           "setup: separation 20M, r 0.75a-13a, beta 10 loop, H/R 0.1 cooling, 1% seeded noise) in "
+                           "the first post-Newtonian binary metric evaluated on the device every substep "
+                           "(metric_dim 3: three time levels, finite-difference connection), COORD_DIAGONAL3 "
+                           "300x160x400, PPM_MC+HLLE+para flux-CT, entropy fix, FP64"),
+    "pnbbh150": dict(kind="pnbbh", n=(150, 80, 200), ref_cfg="pnbbh_dynmink", ref_note=PN_REF_NOTE,
+                     label="pnbbh300 on 150x80x200 zones"),
     "balsara1024": dict(kind="setup", setup="balsara1", n=(1024, 1, 1), ref_cfg="balsara1",
                         label="Balsara-1 shock tube, 1024 zones, MC + HLLE + para flux-CT, CFL 0.5, FP64"),
     "fieldloop512": dict(kind="setup", setup="field_loop", n=(512, 512, 1), ref_cfg="field_loop",
@@ -214,6 +228,22 @@ def setup(wl, device, precision=0, p_init=None):
         e.set_cooling_tables(t["cool_omega"], t["cool_temp"])
         e.upload(p0)
         e.set_time(desc.t, desc.dx[0])
+        return e, p0
+    if wl["kind"] == "pnbbh":
+        from coolharm3d_b200 import pnbbh
+        desc = pnbbh.pnbbh_desc(n, device=device, precision=precision)
+        t = pnbbh.pnbbh_tables(desc)
+        m = pnbbh.pnbbh_coords(spacetime=hg.DYN_PN_BINARY)
+        e = hg.Engine(desc)
+        e.set_dynamic_metric(m)
+        e.set_cell_data(t["cell6"], t["rface"])
+        e.set_cooling_tables(*pnbbh.pn_cooling_tables(t))
+        if p_init is None:
+            p0, _ = pnbbh.set_disk(e, desc, t, m)
+        else:
+            p0 = p_init
+            e.upload(p0)
+        e.set_time(0.0, desc.dx[0])
         return e, p0
     if wl["kind"] == "torus":
         from coolharm3d_b200 import torus
@@ -608,8 +638,8 @@ def reference_arm(wl, ncores, warmup, steps, full_grid=False):
     res = {"value": value, "ms_per_step": 1e3 * slowest / steps, "procs": procs, "block": list(block),
            "build": how, "cpu": _cpu_model(),
            "sample": "%s of the %s grid, one process per core, %d untimed + %d timed steps each "
-                     "(reference CPU build, no MPI halo exchange); %d zones per step" % (
-                         layout, "x".join(map(str, n)), warmup, steps, zones_step)}
+                     "(reference CPU build, no MPI halo exchange); %d zones per step%s" % (
+                         layout, "x".join(map(str, n)), warmup, steps, zones_step, wl.get("ref_note", ""))}
     if full_grid and min(n) > 1:
         v1, s1 = run_reference_blocks(exe, tuple(n), 1, 1, 1)
         if v1 is not None:

@@ -50,7 +50,7 @@ EXPORTS = ["hg_check_mirror", "hg_init", "hg_set_geometry", "hg_set_cell_data", 
            "hg_get_totals", "hg_get_launch_config", "hg_set_launch_config", "hg_autotune",
            "hg_write_rdump", "hg_read_rdump", "hg_fp64_peak", "hg_set_dynamic_metric", "hg_dyn_geometry",
            "hg_dyn_geometry_block", "hg_download_dyn_level"]
-KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc"]
+KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc", "geometry"]
 
 DYN_MINK_SPHERICAL = 2
 DYN_PN_BINARY = 3

@@ -260,7 +260,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     }
     if (G.mdim == 3) {  // three time levels of 42 planes of 5 positions, the substep's connection
       G.gS3 = (long)HG_NPOS * G.S;
-      for (int l = 0; l < 3; l++) ALLOC(G.geomL[l], sizeof(double) * 42 * G.gS3);
+      for (int l = 0; l < 3; l++) ALLOC(G.geomL[l], sizeof(double) * HG_DYN_PLANES * G.gS3);
       ALLOC(G.conn3, sizeof(double) * 64 * G.S);
       ALLOC(G.ctab, sizeof(double) * hg::dyn_tab_layout(G.T).total);
     }
@@ -882,7 +882,7 @@ extern "C" int hg_download_dyn_level(hg_handle *h, int32_t level, double *geom)
   int lev[3];
   HG_CK(copy_sync(h, lev, sc_field(h->G, offsetof(hg::DevScalars, lev)), sizeof(lev), cudaMemcpyDeviceToHost));
   const GridDev &G = h->G;
-  std::vector<double> buf((size_t)42 * G.gS3);
+  std::vector<double> buf((size_t)HG_DYN_PLANES * G.gS3);
   HG_CK(copy_sync(h, buf.data(), G.geomL[lev[level]], sizeof(double) * buf.size(), cudaMemcpyDeviceToHost));
   const long T0 = G.T[0], T1 = G.T[1], T2 = G.T[2];
   for (int pos = 0; pos < HG_NPOS; pos++)
@@ -890,8 +890,19 @@ extern "C" int hg_download_dyn_level(hg_handle *h, int32_t level, double *geom)
       for (long j = 0; j < T1; j++)
         for (long k = 0; k < T2; k++) {
           const long src = (long)pos * G.S + i * G.st[0] + j * G.st[1] + k * G.st[2];
+          auto at = [&](int plane) { return buf[(size_t)plane * G.gS3 + src]; };
           double *o = geom + ((((long)pos * T0 + i) * T1 + j) * T2 + k) * HG_NGEOM;
-          for (int e = 0; e < HG_NGEOM; e++) o[e] = buf[(size_t)e * G.gS3 + src];
+          for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) {
+              o[a * 4 + b] = at(HG_DP_GCON + hg::dyn_sym(a, b));
+              o[16 + a * 4 + b] = at(HG_DP_GCOV + hg::dyn_sym(a, b));
+            }
+          o[32] = at(HG_DP_G);
+          o[33] = at(HG_DP_GINV);
+          o[34] = at(HG_DP_ALPHA);
+          for (int a = 0; a < 3; a++) o[35 + a] = at(HG_DP_BETA + a);
+          o[38] = at(HG_DP_NCON0);
+          for (int a = 1; a < 4; a++) o[38 + a] = -o[34] * o[a];
         }
   return HG_OK;
 }
@@ -1364,7 +1375,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   b += sizeof(hg::DevScalars) + 8ull * cap * (2 + HG_NPR);  // scalars, queue, flagged list
   if (d->use_entropy_eq) b += 8ull * 6 * cap;                 // entropy face fluxes of the queue
   if (d->metric_dim == 2) b += 8ull * 42 * gS + 8ull * 64 * T[0] * T[1];
-  if (d->metric_dim == 3) b += 3ull * 8 * 42 * HG_NPOS * S + 8ull * 64 * S + 8ull * (4 * T[0] + 8 * T[1] + 4 * T[2]);  // coordinate tables
+  if (d->metric_dim == 3) b += 3ull * 8 * HG_DYN_PLANES * HG_NPOS * S + 8ull * 64 * S + 8ull * (4 * T[0] + 8 * T[1] + 4 * T[2]);  // coordinate tables
   if (d->rescale_r) b += 8ull * 12 * T[0];
   if (d->cooling) b += 8ull * 2 * T[0];
   if (d->precision == HG_PREC_MIXED) {

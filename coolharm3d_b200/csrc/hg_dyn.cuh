@@ -277,6 +277,7 @@ HG_DYN_HD void pn_binary(const DynMetric &dm, double t, PNBinary &b)
 // g_cart: with A = 1 + 2V, w = g0i and s = g00 - w.w / A,
 // g^00 = 1/s, g^0i = -w_i / (A s), g^ij = delta_ij / A + w_i w_j / (A^2 s),
 // det g_cart = A^3 s.
+template <bool WITH_GCON = true>
 HG_DYN_HD void pn_metric(const DynMetric &dm, const DynPoint &q, double gcov[4][4], double gcon[4][4],
                          double *gdet)
 {
@@ -310,6 +311,7 @@ HG_DYN_HD void pn_metric(const DynMetric &dm, const DynPoint &q, double gcov[4][
     gcov[a + 1][0] = c;
     for (int e = 0; e < 3; e++) gcov[a + 1][e + 1] = A * (J[a][0] * J[e][0] + J[a][1] * J[e][1] + J[a][2] * J[e][2]);
   }
+  if (!WITH_GCON) return;  // gcov alone: the connection's time derivative
   const double s = g00 - (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]) / A;
   const double iAs = 1. / (A * s);
   double Kw[3];
@@ -373,8 +375,7 @@ HG_DYN_HD void dyn_gcov_func(const GridDev &G, int pos, int i, int j, int k, dou
   DynPoint q;
   dyn_point(G, pos, i, j, k, t, q);
   if (G.dyn.spacetime == HG_DYN_PN_BINARY) {
-    double gcon[4][4], gdet;
-    pn_metric(G.dyn, q, gcov, gcon, &gdet);
+    pn_metric<false>(G.dyn, q, gcov, nullptr, nullptr);
   } else {
     dyn_gcov_sth(q.x, q.sth, gcov);
   }

@@ -109,9 +109,10 @@ struct GridDev {
   long capacity;             // N0*N1*N2
   double *blk;               // per-block partial sums of M_tot
   Geom g0;                   // metric_dim 0 geometry
-  // metric_dim 3: three time levels of geometry, each 42 planes of gS3 =
-  // 5*S doubles (index pos*S + zone offset), filled by k_geom_level; the
-  // connection of the current substep, 64 planes of S (k_conn_dyn)
+  // metric_dim 3: three time levels of geometry, each HG_DYN_PLANES planes
+  // of gS3 = 5*S doubles (index pos*S + zone offset), filled by
+  // k_geom_level; the connection of the current substep, 64 planes of S
+  // (k_conn_dyn)
   double *geomL[3];
   long gS3;
   double *conn3;
@@ -121,6 +122,25 @@ struct GridDev {
   // the platform's libm (dyn_coord_tables, hg_dyn.cuh)
   double *ctab;
 };
+
+// metric_dim 3 level tables: the geometry the engine evaluates is symmetric
+// (gcov[a][b] and gcov[b][a] are the same double), so a struct of_geom is
+// stored as the 10 entries a <= b of gcon and of gcov, g, g_inv, alpha,
+// beta[3] and ncon[0]: 27 planes in place of 42.  ncon[1..3] = -alpha
+// gcon[0][i] are formed on reading with dyn_geom's own operations.
+#define HG_DYN_PLANES 27
+#define HG_DP_GCON 0
+#define HG_DP_GCOV 10
+#define HG_DP_G 20
+#define HG_DP_GINV 21
+#define HG_DP_ALPHA 22
+#define HG_DP_BETA 23
+#define HG_DP_NCON0 26
+__host__ __device__ __forceinline__ int dyn_sym(int a, int b)
+{
+  const int lo = a < b ? a : b, hi = a < b ? b : a;
+  return lo * 4 - (lo * (lo - 1)) / 2 + (hi - lo);  // (0,0)..(0,3) 0..3, (1,1)..(1,3) 4..6, (2,2) 7, (2,3) 8, (3,3) 9
+}
 
 // Fixed grid sizes of the step's kernels (grid-stride loops).
 struct LaunchCfg {
@@ -132,7 +152,7 @@ struct LaunchCfg {
 #define HG_BLK_CAP 65536  // largest grid of any kernel (the per-block M_tot partials are sized for it)
 
 // Kernel classes timed by the optional event recorder.
-enum { KC_FLUX = 0, KC_EMF, KC_UPDATE, KC_FALLBACK, KC_BOUNDS, KC_FIXUP, KC_MISC, KC_END, KC_N };
+enum { KC_FLUX = 0, KC_EMF, KC_UPDATE, KC_FALLBACK, KC_BOUNDS, KC_FIXUP, KC_MISC, KC_GEOM, KC_END, KC_N };
 
 // Optional CUDA-event recorder: an event is recorded on the launch stream
 // before every kernel (tagged with its class) and one after the last.

@@ -1239,15 +1239,15 @@ __global__ void __launch_bounds__(HG_BLK) k_geom_level(GridDev G, int slot, doub
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
-      for (int b = 0; b < 4; b++) {
-        w[(a * 4 + b) * s] = g.gcon[a][b];
-        w[(16 + a * 4 + b) * s] = g.gcov[a][b];
+      for (int b = a; b < 4; b++) {
+        w[(HG_DP_GCON + dyn_sym(a, b)) * s] = g.gcon[a][b];
+        w[(HG_DP_GCOV + dyn_sym(a, b)) * s] = g.gcov[a][b];
       }
-    w[32 * s] = g.g;
-    w[33 * s] = g.g_inv;
-    w[34 * s] = g.alpha;
-    for (int a = 0; a < 3; a++) w[(35 + a) * s] = g.beta[a];
-    for (int a = 0; a < 4; a++) w[(38 + a) * s] = g.ncon[a];
+    w[HG_DP_G * s] = g.g;
+    w[HG_DP_GINV * s] = g.g_inv;
+    w[HG_DP_ALPHA * s] = g.alpha;
+    for (int a = 0; a < 3; a++) w[(HG_DP_BETA + a) * s] = g.beta[a];
+    w[HG_DP_NCON0 * s] = g.ncon[0];
   }
 }
 
@@ -1264,7 +1264,7 @@ __global__ void k_advance_geometry(DevScalars *sc)
 __device__ __forceinline__ double dyn_gcov_at(const GridDev &G, const double *lv, int pos, int i, int j, int k, int a,
                                               int b)
 {
-  return lv[(16 + a * 4 + b) * G.gS3 + (long)pos * G.S + off3(G, i, j, k)];
+  return lv[(HG_DP_GCOV + dyn_sym(a, b)) * G.gS3 + (long)pos * G.S + off3(G, i, j, k)];
 }
 
 // set_general_conn (metric.c:3507-3648) at time t + tfac dx[0] from the
@@ -1295,39 +1295,39 @@ __global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double
   for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
     const unsigned q = e / N0;
     const int i = HG_NGH + (int)(e - q * N0), j = HG_NGH + (int)(q % N1), k = HG_NGH + (int)(q / N1);
-    double c[4][4][4];
+    // dg[sym(a, b)][c] = d_c gcov[a][b]: the stored gcov is symmetric, so the
+    // 40 distinct derivatives stand for conn_func_fd4's 64 (the same values)
+    constexpr int PA[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3}, PB[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+    double dg[10][4];
     {  // time component
       double gh[4][4], gl[4][4];
       dyn_gcov_func(G, 3, i, j, k, t + dtc, gh);
       dyn_gcov_func(G, 3, i, j, k, t - dtc, gl);
 #pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) c[a][b][0] = (gh[a][b] - gl[a][b]) * half_inv_dt_conn;
+      for (int m = 0; m < 10; m++) dg[m][0] = (gh[PA[m]][PB[m]] - gl[PA[m]][PB[m]]) * half_inv_dt_conn;
     }
 #pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-      for (int b = 0; b < 4; b++) {
-        // x1: CENT i-1, FACE1 i, FACE1 i+1, CENT i+1
-        c[a][b][1] = w1[1] * (dyn_gcov_at(G, lv, 3, i - 1, j, k, a, b) - dyn_gcov_at(G, lv, 3, i + 1, j, k, a, b)) +
-                     w2[1] * (dyn_gcov_at(G, lv, 0, i + 1, j, k, a, b) - dyn_gcov_at(G, lv, 0, i, j, k, a, b));
-        if (phys2 && j == N2S) {
-          c[a][b][2] = w_2lo[0] * dyn_gcov_at(G, lv, 1, i, j, k, a, b) + w_2lo[1] * dyn_gcov_at(G, lv, 3, i, j, k, a, b) +
-                       w_2lo[2] * dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b) +
-                       w_2lo[3] * dyn_gcov_at(G, lv, 3, i, j + 1, k, a, b) +
-                       w_2lo[4] * dyn_gcov_at(G, lv, 1, i, j + 2, k, a, b);
-        } else if (phys2 && j == N2E) {
-          c[a][b][2] = w_2hi[0] * dyn_gcov_at(G, lv, 1, i, j - 1, k, a, b) +
-                       w_2hi[1] * dyn_gcov_at(G, lv, 3, i, j - 1, k, a, b) + w_2hi[2] * dyn_gcov_at(G, lv, 1, i, j, k, a, b) +
-                       w_2hi[3] * dyn_gcov_at(G, lv, 3, i, j, k, a, b) + w_2hi[4] * dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b);
-        } else {
-          c[a][b][2] = w1[2] * (dyn_gcov_at(G, lv, 3, i, j - 1, k, a, b) - dyn_gcov_at(G, lv, 3, i, j + 1, k, a, b)) +
-                       w2[2] * (dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b) - dyn_gcov_at(G, lv, 1, i, j, k, a, b));
-        }
-        c[a][b][3] = w1[3] * (dyn_gcov_at(G, lv, 3, i, j, k - 1, a, b) - dyn_gcov_at(G, lv, 3, i, j, k + 1, a, b)) +
-                     w2[3] * (dyn_gcov_at(G, lv, 2, i, j, k + 1, a, b) - dyn_gcov_at(G, lv, 2, i, j, k, a, b));
+    for (int m = 0; m < 10; m++) {
+      const int a = PA[m], b = PB[m];
+      // x1: CENT i-1, FACE1 i, FACE1 i+1, CENT i+1
+      dg[m][1] = w1[1] * (dyn_gcov_at(G, lv, 3, i - 1, j, k, a, b) - dyn_gcov_at(G, lv, 3, i + 1, j, k, a, b)) +
+                 w2[1] * (dyn_gcov_at(G, lv, 0, i + 1, j, k, a, b) - dyn_gcov_at(G, lv, 0, i, j, k, a, b));
+      if (phys2 && j == N2S) {
+        dg[m][2] = w_2lo[0] * dyn_gcov_at(G, lv, 1, i, j, k, a, b) + w_2lo[1] * dyn_gcov_at(G, lv, 3, i, j, k, a, b) +
+                   w_2lo[2] * dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b) +
+                   w_2lo[3] * dyn_gcov_at(G, lv, 3, i, j + 1, k, a, b) +
+                   w_2lo[4] * dyn_gcov_at(G, lv, 1, i, j + 2, k, a, b);
+      } else if (phys2 && j == N2E) {
+        dg[m][2] = w_2hi[0] * dyn_gcov_at(G, lv, 1, i, j - 1, k, a, b) +
+                   w_2hi[1] * dyn_gcov_at(G, lv, 3, i, j - 1, k, a, b) + w_2hi[2] * dyn_gcov_at(G, lv, 1, i, j, k, a, b) +
+                   w_2hi[3] * dyn_gcov_at(G, lv, 3, i, j, k, a, b) + w_2hi[4] * dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b);
+      } else {
+        dg[m][2] = w1[2] * (dyn_gcov_at(G, lv, 3, i, j - 1, k, a, b) - dyn_gcov_at(G, lv, 3, i, j + 1, k, a, b)) +
+                   w2[2] * (dyn_gcov_at(G, lv, 1, i, j + 1, k, a, b) - dyn_gcov_at(G, lv, 1, i, j, k, a, b));
       }
+      dg[m][3] = w1[3] * (dyn_gcov_at(G, lv, 3, i, j, k - 1, a, b) - dyn_gcov_at(G, lv, 3, i, j, k + 1, a, b)) +
+                 w2[3] * (dyn_gcov_at(G, lv, 2, i, j, k + 1, a, b) - dyn_gcov_at(G, lv, 2, i, j, k, a, b));
+    }
     // DGCOV_TO_CONN with tmp[l][b][cc] formed where it is used (the same
     // operations, without a second 64-entry array per thread)
     const long o = off3(G, i, j, k);
@@ -1336,7 +1336,7 @@ __global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
-      for (int l = 0; l < 4; l++) gcon[a][l] = lv[(a * 4 + l) * G.gS3 + oc];
+      for (int l = 0; l < 4; l++) gcon[a][l] = lv[(HG_DP_GCON + dyn_sym(a, l)) * G.gS3 + oc];
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -1345,7 +1345,8 @@ __global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double
         for (int cc = 0; cc < 4; cc++) {
           double v = 0.;
 #pragma unroll
-          for (int l = 0; l < 4; l++) v += gcon[a][l] * (0.5 * (c[b][l][cc] + c[cc][l][b] - c[cc][b][l]));
+          for (int l = 0; l < 4; l++)
+            v += gcon[a][l] * (0.5 * (dg[dyn_sym(b, l)][cc] + dg[dyn_sym(cc, l)][b] - dg[dyn_sym(cc, b)][l]));
           G.conn3[((a * 4 + b) * 4 + cc) * G.S + o] = v;
         }
   }
@@ -1483,7 +1484,10 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
   k_begin<<<1, 1, 0, s>>>(G.sc);
   // set_general_conn(t) before the predictor, set_general_conn(t + dx[0]/2)
   // before the corrector (step_ch.c:79-83, 128-133), from ncurr's level
-  if (G.mdim == 3) k_conn_dyn<<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, 0.5 * sub);
+  if (G.mdim == 3) {
+    mark(R, KC_GEOM, s);
+    k_conn_dyn<<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, 0.5 * sub);
+  }
   // (the mixed form's FP32 copy of ph is already current: put_state)
   for (int d = 0; d < 3; d++) launch_flux_dir(G, L, s, ph, d, R, sub);
   {
@@ -1713,7 +1717,7 @@ __device__ __forceinline__ double divb_zone(const GridDev &G, int i, int j, int 
         if (G.mdim == 0) g = G.g0.g;
         else if (G.mdim == 3) {
           const int L = G.sc->lev[0];
-          g = (L == 0 ? G.geomL[0] : L == 1 ? G.geomL[1] : G.geomL[2])[32 * G.gS3 + 3 * G.S + o];
+          g = (L == 0 ? G.geomL[0] : L == 1 ? G.geomL[1] : G.geomL[2])[HG_DP_G * G.gS3 + 3 * G.S + o];
         } else
           g = G.geomT[32 * G.gS + ((long)3 * G.T[1] + (G.deg[1] ? 0 : j + dj)) * G.T[0] + (G.deg[0] ? 0 : i + di)];
         const double b1 = G.p[B1 * G.S + o], b2 = G.p[B2 * G.S + o], b3 = G.p[B3 * G.S + o];
@@ -1834,6 +1838,7 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
   mark(R, KC_MISC, s);
   k_timestep<<<1, 1024, 0, s>>>(G, L.grid_upd);
   if (G.mdim == 3) {  // advance_geometry() at the end of step_ch() (step_ch.c:225-227)
+    mark(R, KC_GEOM, s);
     k_advance_geometry<<<1, 1, 0, s>>>(G.sc);
     launch_geom_level(G, L, s, 1, 0.5);
     launch_geom_level(G, L, s, 2, 1.0);

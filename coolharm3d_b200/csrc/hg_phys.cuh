@@ -52,6 +52,27 @@ __device__ __forceinline__ void load_geom(const GridDev &G, int pos, int i, int 
     const int L = G.sc->lev[slot];
     t = (L == 0 ? G.geomL[0] : L == 1 ? G.geomL[1] : G.geomL[2]) + (long)pos * G.S + off3(G, i, j, k);
     s = G.gS3;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = a; b < 4; b++) {
+        const double cn = __ldg(t + (HG_DP_GCON + dyn_sym(a, b)) * s), cv = __ldg(t + (HG_DP_GCOV + dyn_sym(a, b)) * s);
+        g.gcon[a][b] = cn;
+        g.gcon[b][a] = cn;
+        g.gcov[a][b] = cv;
+        g.gcov[b][a] = cv;
+      }
+    g.g = __ldg(t + HG_DP_G * s);
+    g.g_inv = __ldg(t + HG_DP_GINV * s);
+    g.alpha = __ldg(t + HG_DP_ALPHA * s);
+    g.beta[0] = __ldg(t + (HG_DP_BETA + 0) * s);
+    g.beta[1] = __ldg(t + (HG_DP_BETA + 1) * s);
+    g.beta[2] = __ldg(t + (HG_DP_BETA + 2) * s);
+    g.ncon[0] = __ldg(t + HG_DP_NCON0 * s);
+    g.ncon[1] = -g.alpha * g.gcon[0][1];
+    g.ncon[2] = -g.alpha * g.gcon[0][2];
+    g.ncon[3] = -g.alpha * g.gcon[0][3];
+    return;
   } else {
     const int ii = G.deg[0] ? 0 : i, jj = G.deg[1] ? 0 : j;
     const long o = ((long)pos * G.T[1] + jj) * G.T[0] + ii;

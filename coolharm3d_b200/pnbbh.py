@@ -190,6 +190,29 @@ def _radius_of_r(r, r0=0.0):
     return r0 + math.exp(math.log(r - r0))
 
 
+def _sqrt(x):
+    """C's sqrt: NaN for a negative argument (rho_func's radicands go negative
+    near the axis; the NaN then fails h > 1 and the zone is outside the disk)."""
+    return math.sqrt(x) if x >= 0. else math.nan
+
+
+def _pow(x, y):
+    """C's pow for the cases rho_func meets: NaN propagates, a negative base
+    with a non-integer exponent gives NaN."""
+    try:
+        return math.pow(x, y)
+    except ValueError:
+        return math.nan
+
+
+def _div(a, b):
+    """C's division of doubles: a zero divisor gives +-inf or NaN."""
+    try:
+        return a / b
+    except ZeroDivisionError:
+        return math.nan if (a == 0. or a != a) else math.copysign(math.inf, a) * math.copysign(1., b)
+
+
 class _Disk:
     """rho_func, get_rpmax, find_l_bracket, find_l_ang_in with the reference's
     shared state (init.nz_pn_bbh_disk.c:668-974)."""
@@ -213,23 +236,23 @@ class _Disk:
         q, gam = self.q, self.gam
         gi = self.geom_in[1]
         sign_l = 1. if l_in >= 0. else -1.
-        lambda_in = math.sqrt(-gi[3] / gi[5])
-        eta = abs(l_in) * math.pow(lambda_in, (q - 2.))
-        eta_2q = sign_l * math.pow(eta, 2. / q)
-        k_eta = math.pow(eta, (-2. / (q - 2.)))
-        f_l_in = math.pow(abs(1. - k_eta * math.pow(l_in, self.exp_4)), self.exp_2)
-        utcov_in = -1. / math.sqrt(-gi[3] + l_in * (2 * gi[4] - l_in * gi[5]))
-        lam = math.sqrt(-g[3] / g[5])
-        omega = eta * math.pow(lam, -q)
-        l_ang = eta_2q * math.pow(omega, self.exp_3)
-        f_l = math.pow(abs(1. - k_eta * math.pow(l_ang, self.exp_4)), self.exp_2)
-        utcov = -1. / math.sqrt(-g[3] + l_ang * (2 * g[4] - l_ang * g[5]))
-        utcon = 1. / math.sqrt(-(g[0] + omega * (2. * g[1] + omega * g[2])))
+        lambda_in = _sqrt(-gi[3] / gi[5])
+        eta = abs(l_in) * _pow(lambda_in, (q - 2.))
+        eta_2q = sign_l * _pow(eta, 2. / q)
+        k_eta = _pow(eta, (-2. / (q - 2.)))
+        f_l_in = _pow(abs(1. - k_eta * _pow(l_in, self.exp_4)), self.exp_2)
+        utcov_in = _div(-1., _sqrt(-gi[3] + l_in * (2 * gi[4] - l_in * gi[5])))
+        lam = _sqrt(-g[3] / g[5])
+        omega = eta * _pow(lam, -q)
+        l_ang = eta_2q * _pow(omega, self.exp_3)
+        f_l = _pow(abs(1. - k_eta * _pow(l_ang, self.exp_4)), self.exp_2)
+        utcov = _div(-1., _sqrt(-g[3] + l_ang * (2 * g[4] - l_ang * g[5])))
+        utcon = _div(1., _sqrt(-(g[0] + omega * (2. * g[1] + omega * g[2]))))
         upcon = omega * utcon
-        h = utcov_in * f_l_in / (utcov * f_l)
+        h = _div(utcov_in * f_l_in, utcov * f_l)
         if h > 1. and xr > self.rin:
             eps = (h - 1.) / gam
-            rho = math.pow((eps * (gam - 1.) / self.adiab), (1. / (gam - 1.)))
+            rho = _pow((eps * (gam - 1.) / self.adiab), (1. / (gam - 1.)))
             uu = rho * eps * (1. + self.grscale * (self.ranc() - 0.5))
         else:
             rho = uu = -1.
@@ -483,7 +506,8 @@ def set_disk(target, desc, tables, metric, beta=10.0, seed=1, t0=0.0, return_pri
                       rk[i0 - 1:i1 - 1, j0 - 1:j1 - 1])
     rho_cut = 0.25 * h["rho_max"]
     A = np.where(rho_avg > rho_cut, rho_avg - rho_cut, 0.0)
-    geo0 = dyn_geometry_block(desc, metric, CENT, t0, NG, n1)[:, NG:NG + n2, 0]
+    geo0 = np.concatenate([dyn_geometry_block(desc, metric, CENT, t0, NG + i0, min(plane_batch, n1 - i0))[:, NG:NG + n2, 0]
+                           for i0 in range(0, n1, plane_batch)])
     gdet = geo0[..., G_G]
     b1 = -(A[:-1, :-1] - A[:-1, 1:] + A[1:, :-1] - A[1:, 1:]) / (2. * desc.dx[2] * gdet)
     b2 = (A[:-1, :-1] + A[:-1, 1:] - A[1:, :-1] - A[1:, 1:]) / (2. * desc.dx[1] * gdet)

@@ -285,10 +285,11 @@ int hg_last_step_ms(hg_handle *h, double *ms);
 /* Per-kernel timing.  hg_profile(h, 1) makes every following hg_step record a
  * CUDA event on the engine's stream before each kernel; hg_kernel_times()
  * returns, per kernel class (flux, emf, update, fallback, bounds, fixup,
- * misc), the summed milliseconds and the number of launches since the last
+ * misc, geometry -- the time levels and connection of metric_dim 3), the
+ * summed milliseconds and the number of launches since the last
  * hg_profile() call.  The reference has no counterpart (it times with
  * gettimeofday around whole routines, macros.h:620-657). */
-#define HG_NKCLASS 7
+#define HG_NKCLASS 8
 int hg_profile(hg_handle *h, int32_t enable);
 int hg_kernel_times(hg_handle *h, double ms[HG_NKCLASS], int64_t launches[HG_NKCLASS]);
 
