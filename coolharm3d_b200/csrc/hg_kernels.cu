@@ -319,7 +319,8 @@ __device__ __forceinline__ void strip_recon(const GridDev &G, const double *__re
 template <bool RS, int MDIM, int d, int NF>
 __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux_strip(const __grid_constant__ GridDev G,
                                                                    const double *__restrict__ ph, int lo0, int lo1,
-                                                                   int lo2, int n0, int n1, int n2, unsigned int mult)
+                                                                   int lo2, int n0, int n1, int n2, unsigned int mult,
+                                                                   int slot)
 {
   extern __shared__ double sm[];  // 16 * NF * HG_BLK doubles: the strip's face states
   const int tx = threadIdx.x;
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX_MINB) k_flux_strip(const __gri
         ctop = face_flux(G, pl, pr, G.g0, d, i, j, k, mult, G.F[d], o);
       } else {
         Geom g;
-        load_geom(G, d, i, j, g);
+        load_geom(G, d, i, j, g, k, slot);  // metric_dim 3: time level `slot`
         ctop = face_flux(G, pl, pr, g, d, i, j, k, mult, G.F[d], o);
       }
       if (d == 0 && G.bc == 10) {  // fix_flux(), bounds.c:2263-2275: no mass inflow through r_in, r_out
@@ -1374,10 +1375,11 @@ static inline void mark(EventRec *r, int cls, cudaStream_t s)
 // torus NF = 2 measured best, and hg_autotune chooses per grid.
 template <bool RS, int MDIM, int d, int NF>
 static void launch_strip_nf(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, const int *lo,
-                            const int *n, unsigned int mult)
+                            const int *n, unsigned int mult, int slot)
 {
   const size_t smem = sizeof(double) * 16 * NF * HG_BLK;
-  k_flux_strip<RS, MDIM, d, NF><<<L.grid_flux, HG_BLK, smem, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult);
+  k_flux_strip<RS, MDIM, d, NF>
+      <<<L.grid_flux, HG_BLK, smem, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult, slot);
 }
 
 template <bool RS, int MDIM, int d, int NF>
@@ -1404,19 +1406,21 @@ static cudaError_t strip_attrs_rm()
 // stream capture: called by hg_init.
 cudaError_t prepare_kernels()
 {
-  cudaError_t e = strip_attrs_rm<false, 0>();
-  const cudaError_t e1 = strip_attrs_rm<true, 0>(), e2 = strip_attrs_rm<false, 2>(), e3 = strip_attrs_rm<true, 2>();
-  return e != cudaSuccess ? e : e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3;
+  const cudaError_t r[6] = {strip_attrs_rm<false, 0>(), strip_attrs_rm<true, 0>(), strip_attrs_rm<false, 2>(),
+                            strip_attrs_rm<true, 2>(),  strip_attrs_rm<false, 3>(), strip_attrs_rm<true, 3>()};
+  for (cudaError_t x : r)
+    if (x != cudaSuccess) return x;
+  return cudaSuccess;
 }
 
 // strips of L.strip_nf faces (1, 2 or 3: a launch-configuration choice)
 template <bool RS, int MDIM, int d>
 static void launch_strip(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, const int *lo,
-                         const int *n, unsigned int mult)
+                         const int *n, unsigned int mult, int slot)
 {
-  if (L.strip_nf <= 1) launch_strip_nf<RS, MDIM, d, 1>(G, L, s, ph, lo, n, mult);
-  else if (L.strip_nf == 2) launch_strip_nf<RS, MDIM, d, 2>(G, L, s, ph, lo, n, mult);
-  else launch_strip_nf<RS, MDIM, d, 3>(G, L, s, ph, lo, n, mult);
+  if (L.strip_nf <= 1) launch_strip_nf<RS, MDIM, d, 1>(G, L, s, ph, lo, n, mult, slot);
+  else if (L.strip_nf == 2) launch_strip_nf<RS, MDIM, d, 2>(G, L, s, ph, lo, n, mult, slot);
+  else launch_strip_nf<RS, MDIM, d, 3>(G, L, s, ph, lo, n, mult, slot);
 }
 
 static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ph, int d,
@@ -1448,7 +1452,7 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
 #define HG_FLUX(RSV, MD, DD) \
   k_flux<RSV, MD, DD><<<L.grid_flux, HG_BLK, 0, s>>>(G, ph, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult, slot)
 #define HG_STRIP(RSV, MD, DD) \
-  launch_strip<RSV, MD, DD>(G, L, s, ph, lo, n, mult)
+  launch_strip<RSV, MD, DD>(G, L, s, ph, lo, n, mult, slot)
 #define HG_FLUX_D(RSV, MD) \
   if (d == 0) { if (G.deg[0] || !L.strip_x1) HG_FLUX(RSV, MD, 0); else HG_STRIP(RSV, MD, 0); } \
   else if (d == 1) { if (G.deg[1]) HG_FLUX(RSV, MD, 1); else HG_STRIP(RSV, MD, 1); } \
@@ -1456,16 +1460,9 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
     if (G.mdim == 0) {
       if (G.rescale) { HG_FLUX_D(true, 0) }
       else { HG_FLUX_D(false, 0) }
-    } else if (G.mdim == 3) {  // one face per thread, geometry of time level `slot`
-      if (G.rescale) {
-        if (d == 0) HG_FLUX(true, 3, 0);
-        else if (d == 1) HG_FLUX(true, 3, 1);
-        else HG_FLUX(true, 3, 2);
-      } else {
-        if (d == 0) HG_FLUX(false, 3, 0);
-        else if (d == 1) HG_FLUX(false, 3, 1);
-        else HG_FLUX(false, 3, 2);
-      }
+    } else if (G.mdim == 3) {  // geometry of time level `slot`
+      if (G.rescale) { HG_FLUX_D(true, 3) }
+      else { HG_FLUX_D(false, 3) }
     } else {
       if (G.rescale) { HG_FLUX_D(true, 2) }
       else { HG_FLUX_D(false, 2) }
