@@ -96,6 +96,8 @@ WORKLOADS = {
                            "300x160x400, PPM_MC+HLLE+para flux-CT, entropy fix, FP64"),
     "pnbbh150": dict(kind="pnbbh", n=(150, 80, 200), ref_cfg="pnbbh_dynmink", ref_note=PN_REF_NOTE,
                      label="pnbbh300 on 150x80x200 zones"),
+    "pnbbh75": dict(kind="pnbbh", n=(75, 40, 100), ref_cfg="pnbbh_dynmink", ref_note=PN_REF_NOTE,
+                    label="pnbbh300 on 75x40x100 zones (profiling size)"),
     "balsara1024": dict(kind="setup", setup="balsara1", n=(1024, 1, 1), ref_cfg="balsara1",
                         label="Balsara-1 shock tube, 1024 zones, MC + HLLE + para flux-CT, CFL 0.5, FP64"),
     "fieldloop512": dict(kind="setup", setup="field_loop", n=(512, 512, 1), ref_cfg="field_loop",

@@ -305,8 +305,9 @@ class Engine:
 
     def dyn_level(self, level=0):
         """metric_dim 3: time level 0/1/2 (n_beg, n_mid, n_end) of the next
-        step as the device evaluated it, (5, N1TOT, N2TOT, N3TOT, 42)."""
-        out = np.empty((5,) + self.shape + (NGEOM,))
+        step as the device evaluated it, (4, N1TOT, N2TOT, N3TOT, 42): the
+        positions FACE1..FACE3 and CENT."""
+        out = np.empty((4,) + self.shape + (NGEOM,))
         _check(self.lib.hg_download_dyn_level(self.h, level, _ptr(out)), "hg_download_dyn_level")
         return out
 

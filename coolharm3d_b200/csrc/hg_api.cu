@@ -259,7 +259,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
       ALLOC(G.conn, sizeof(double) * 64 * G.T[0] * G.T[1]);
     }
     if (G.mdim == 3) {  // three time levels of 42 planes of 5 positions, the substep's connection
-      G.gS3 = (long)HG_NPOS * G.S;
+      G.gS3 = (long)HG_DYN_NPOS * G.S;
       for (int l = 0; l < 3; l++) ALLOC(G.geomL[l], sizeof(double) * HG_DYN_PLANES * G.gS3);
       ALLOC(G.conn3, sizeof(double) * 64 * G.S);
       ALLOC(G.ctab, sizeof(double) * hg::dyn_tab_layout(G.T).total);
@@ -885,7 +885,7 @@ extern "C" int hg_download_dyn_level(hg_handle *h, int32_t level, double *geom)
   std::vector<double> buf((size_t)HG_DYN_PLANES * G.gS3);
   HG_CK(copy_sync(h, buf.data(), G.geomL[lev[level]], sizeof(double) * buf.size(), cudaMemcpyDeviceToHost));
   const long T0 = G.T[0], T1 = G.T[1], T2 = G.T[2];
-  for (int pos = 0; pos < HG_NPOS; pos++)
+  for (int pos = 0; pos < HG_DYN_NPOS; pos++)
     for (long i = 0; i < T0; i++)
       for (long j = 0; j < T1; j++)
         for (long k = 0; k < T2; k++) {
@@ -1375,7 +1375,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   b += sizeof(hg::DevScalars) + 8ull * cap * (2 + HG_NPR);  // scalars, queue, flagged list
   if (d->use_entropy_eq) b += 8ull * 6 * cap;                 // entropy face fluxes of the queue
   if (d->metric_dim == 2) b += 8ull * 42 * gS + 8ull * 64 * T[0] * T[1];
-  if (d->metric_dim == 3) b += 3ull * 8 * HG_DYN_PLANES * HG_NPOS * S + 8ull * 64 * S + 8ull * (4 * T[0] + 8 * T[1] + 4 * T[2]);  // coordinate tables
+  if (d->metric_dim == 3) b += 3ull * 8 * HG_DYN_PLANES * HG_DYN_NPOS * S + 8ull * 64 * S + 8ull * (4 * T[0] + 8 * T[1] + 4 * T[2]);  // coordinate tables
   if (d->rescale_r) b += 8ull * 12 * T[0];
   if (d->cooling) b += 8ull * 2 * T[0];
   if (d->precision == HG_PREC_MIXED) {

@@ -278,18 +278,15 @@ HG_DYN_HD void pn_binary(const DynMetric &dm, double t, PNBinary &b)
 // g^00 = 1/s, g^0i = -w_i / (A s), g^ij = delta_ij / A + w_i w_j / (A^2 s),
 // det g_cart = A^3 s.
 template <bool WITH_GCON = true>
-HG_DYN_HD void pn_metric(const DynMetric &dm, const DynPoint &q, double gcov[4][4], double gcon[4][4],
-                         double *gdet)
+HG_DYN_HD void pn_metric(const PNBinary &b, const DynPoint &q, double gcov[4][4], double gcon[4][4], double *gdet,
+                         double *s_out)
 {
-  PNBinary b;
-  pn_binary(dm, q.x[0], b);
   const double r = q.x[1];
   const double X[3] = {r * q.sth * q.cph, r * q.sth * q.sph, r * q.cth};
   double V = 0., Vi[3] = {0., 0., 0.};
   for (int a = 0; a < 2; a++) {
     const double d0 = X[0] - b.y[a][0], d1 = X[1] - b.y[a][1], d2 = X[2] - b.y[a][2];
-    const double ra = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-    const double ma = b.m[a] / ra;
+    const double ma = b.m[a] / sqrt(d0 * d0 + d1 * d1 + d2 * d2);
     V += ma;
     for (int c = 0; c < 3; c++) Vi[c] += ma * b.v[a][c];
   }
@@ -312,29 +309,56 @@ HG_DYN_HD void pn_metric(const DynMetric &dm, const DynPoint &q, double gcov[4][
     for (int e = 0; e < 3; e++) gcov[a + 1][e + 1] = A * (J[a][0] * J[e][0] + J[a][1] * J[e][1] + J[a][2] * J[e][2]);
   }
   if (!WITH_GCON) return;  // gcov alone: the connection's time derivative
-  const double s = g00 - (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]) / A;
-  const double iAs = 1. / (A * s);
+  const double iA = 1. / A;
+  const double s = g00 - (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]) * iA;
+  const double is = 1. / s, iAs = iA * is;
   double Kw[3];
   for (int a = 0; a < 3; a++) Kw[a] = K[a][0] * w[0] + K[a][1] * w[1] + K[a][2] * w[2];
-  gcon[0][0] = 1. / s;
+  gcon[0][0] = is;
   for (int a = 0; a < 3; a++) {
     gcon[0][a + 1] = -Kw[a] * iAs;
     gcon[a + 1][0] = gcon[0][a + 1];
     for (int e = 0; e < 3; e++)
-      gcon[a + 1][e + 1] = (K[a][0] * K[e][0] + K[a][1] * K[e][1] + K[a][2] * K[e][2]) / A + Kw[a] * Kw[e] * iAs / A;
+      gcon[a + 1][e + 1] = (K[a][0] * K[e][0] + K[a][1] * K[e][1] + K[a][2] * K[e][2]) * iA + Kw[a] * Kw[e] * iAs * iA;
   }
   *gdet = sqrt(-(A * A * A * s)) * fabs(q.det * r * r * q.sth);
+  *s_out = s;
 }
 
 // The struct of_geom of one position at time t: set_general_geometry's loop
 // body (metric.c:3453-3483) with transform_all (coord.c:2340-2355:
 // transform_rank2cov2 / transform_rank2con2, coord.c:1852-1879, 1975-2002).
-HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t, Geom &g)
+// bin: the PN binary at time t when the caller has it (kernels evaluate it
+// once per level), else it is evaluated here.
+HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t, Geom &g,
+                        const PNBinary *bin = nullptr)
 {
   DynPoint q;
   dyn_point(G, pos, i, j, k, t, q);
   if (G.dyn.spacetime == HG_DYN_PN_BINARY) {
-    pn_metric(G.dyn, q, g.gcov, g.gcon, &g.g);
+    PNBinary b0;
+    if (!bin) {
+      pn_binary(G.dyn, t, b0);
+      bin = &b0;
+    }
+    double s;
+    pn_metric(*bin, q, g.gcov, g.gcon, &g.g, &s);
+    // the derived quantities of set_general_geometry, with 1/gcon[0][0] = s
+    g.g_inv = 1. / g.g;
+    double inv00 = s;
+    if (g.gcon[0][0] >= HG_GCON_EPS) {
+      g.gcon[0][0] = HG_GCON_EPS;
+      inv00 = 1. / HG_GCON_EPS;
+    }
+    g.ncon[0] = sqrt(-g.gcon[0][0]);
+    g.alpha = 1. / g.ncon[0];
+    g.ncon[1] = -g.alpha * g.gcon[0][1];
+    g.ncon[2] = -g.alpha * g.gcon[0][2];
+    g.ncon[3] = -g.alpha * g.gcon[0][3];
+    g.beta[0] = -g.gcon[0][1] * inv00;
+    g.beta[1] = -g.gcon[0][2] * inv00;
+    g.beta[2] = -g.gcon[0][3] * inv00;
+    return;
   } else {
   double gc[4][4], gn[4][4];
   dyn_gcov_sth(q.x, q.sth, gc);
@@ -370,12 +394,18 @@ HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t
 // spacetime in the grid's own (spherical) topology is not transformed there;
 // a Cartesian one -- the PN binary -- is taken to the numerical coordinates
 // (transform_rank2cov2 with dxc_dxp, metric.c:3968-3976).
-HG_DYN_HD void dyn_gcov_func(const GridDev &G, int pos, int i, int j, int k, double t, double gcov[4][4])
+HG_DYN_HD void dyn_gcov_func(const GridDev &G, int pos, int i, int j, int k, double t, double gcov[4][4],
+                             const PNBinary *bin = nullptr)
 {
   DynPoint q;
   dyn_point(G, pos, i, j, k, t, q);
   if (G.dyn.spacetime == HG_DYN_PN_BINARY) {
-    pn_metric<false>(G.dyn, q, gcov, nullptr, nullptr);
+    PNBinary b0;
+    if (!bin) {
+      pn_binary(G.dyn, t, b0);
+      bin = &b0;
+    }
+    pn_metric<false>(*bin, q, gcov, nullptr, nullptr, nullptr);
   } else {
     dyn_gcov_sth(q.x, q.sth, gcov);
   }

@@ -129,6 +129,9 @@ struct GridDev {
 // beta[3] and ncon[0]: 27 planes in place of 42.  ncon[1..3] = -alpha
 // gcon[0][i] are formed on reading with dyn_geom's own operations.
 #define HG_DYN_PLANES 27
+// positions kept per level: FACE1, FACE2, FACE3, CENT (no kernel reads the
+// corner position's geometry)
+#define HG_DYN_NPOS 4
 #define HG_DP_GCON 0
 #define HG_DP_GCOV 10
 #define HG_DP_G 20

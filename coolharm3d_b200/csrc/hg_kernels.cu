@@ -1228,13 +1228,19 @@ __global__ void __launch_bounds__(HG_BLK) k_geom_level(GridDev G, int slot, doub
 {
   double *out = dyn_level(G, slot);
   const double t = G.sc->t + tfac * G.sc->dt;
+  const bool pn = G.dyn.spacetime == HG_DYN_PN_BINARY;
+  __shared__ PNBinary bin;  // the binary at the level's time, once per block
+  if (pn) {
+    if (threadIdx.x == 0) pn_binary(G.dyn, t, bin);
+    __syncthreads();
+  }
   const unsigned T0 = G.T[0], T1 = G.T[1];
-  const unsigned total = 5u * (unsigned)G.S;  // < 2^31 (hg_init's bound on 5 planes)
+  const unsigned total = (unsigned)HG_DYN_NPOS * (unsigned)G.S;  // < 2^31 (hg_init's bound on 5 planes)
   for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
     const unsigned pos = e / (unsigned)G.S, o = e - pos * (unsigned)G.S;
     const int i = (int)(o % T0), j = (int)((o / T0) % T1), k = (int)(o / (T0 * T1));
     Geom g;
-    dyn_geom(G, (int)pos, i, j, k, t, g);
+    dyn_geom(G, (int)pos, i, j, k, t, g, pn ? &bin : nullptr);
     double *w = out + e;
     const long s = G.gS3;
 #pragma unroll
@@ -1281,6 +1287,12 @@ __global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double
   const double *lv = dyn_level(G, slot);
   const double t = G.sc->t + tfac * G.sc->dt;
   const double dtc = G.dyn.dt_conn, half_inv_dt_conn = 0.5 / dtc;
+  const bool pn = G.dyn.spacetime == HG_DYN_PN_BINARY;
+  __shared__ PNBinary bhl[2];  // the binary at t + dt_conn and t - dt_conn, once per block
+  if (pn) {
+    if (threadIdx.x < 2) pn_binary(G.dyn, threadIdx.x == 0 ? t + dtc : t - dtc, bhl[threadIdx.x]);
+    __syncthreads();
+  }
   const unsigned N0 = G.N[0], N1 = G.N[1];
   const unsigned total = (unsigned)G.capacity;
   const bool phys2 = (G.bc != 1);  // x2 boundaries physical (not periodic)
@@ -1302,8 +1314,8 @@ __global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double
     double dg[10][4];
     {  // time component
       double gh[4][4], gl[4][4];
-      dyn_gcov_func(G, 3, i, j, k, t + dtc, gh);
-      dyn_gcov_func(G, 3, i, j, k, t - dtc, gl);
+      dyn_gcov_func(G, 3, i, j, k, t + dtc, gh, pn ? &bhl[0] : nullptr);
+      dyn_gcov_func(G, 3, i, j, k, t - dtc, gl, pn ? &bhl[1] : nullptr);
 #pragma unroll
       for (int m = 0; m < 10; m++) dg[m][0] = (gh[PA[m]][PB[m]] - gl[PA[m]][PB[m]]) * half_inv_dt_conn;
     }

@@ -158,7 +158,9 @@ int hg_dyn_geometry_block(const hg_grid_desc *desc, const hg_dyn_metric *m, int3
 /* metric_dim 3: the time level `level` (0 n_beg, 1 n_mid, 2 n_end) of the
  * step about to run, as the device evaluated it, in the reference's layout
  * out[(((pos*N1TOT + i)*N2TOT + j)*N3TOT + k)*HG_NGEOM + e] (the geom_arr of
- * METRIC_DIM 3, decomp.c:168): for checking the device's evaluation. */
+ * METRIC_DIM 3, decomp.c:168) for the positions 0..3 (FACE1..FACE3, CENT;
+ * no kernel reads the corner's, so the device does not evaluate it): for
+ * checking the device's evaluation. */
 int hg_download_dyn_level(hg_handle *h, int32_t level, double *geom);
 
 /* Primitive variables in the reference layout (flattened p[i][j][k][l]).

@@ -126,7 +126,7 @@ def test_device_levels_match_host(spacetime):
     e.set_time(t0, dt)
     for lev, tl in ((0, t0), (1, t0 + 0.5 * dt), (2, t0 + dt)):
         dev = e.dyn_level(lev)
-        host = np.stack([hg.dyn_geometry_block(d, m, pos, tl, 0, e.shape[0]) for pos in range(5)])
+        host = np.stack([hg.dyn_geometry_block(d, m, pos, tl, 0, e.shape[0]) for pos in range(4)])
         if spacetime == "mink":
             assert np.array_equal(dev, host), lev
         else:
