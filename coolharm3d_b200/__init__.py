@@ -52,6 +52,7 @@ EXPORTS = ["hg_check_mirror", "hg_init", "hg_set_geometry", "hg_set_cell_data", 
            "hg_dyn_geometry_block", "hg_download_dyn_level"]
 KERNEL_CLASSES = ["flux", "emf", "update", "fallback", "bounds", "fixup", "misc", "geometry"]
 
+DYN_KS_SPHERICAL = 0
 DYN_MINK_SPHERICAL = 2
 DYN_PN_BINARY = 3
 
@@ -62,14 +63,16 @@ class DynMetric(ctypes.Structure):
     _fields_ = [("spacetime", ctypes.c_int32), ("diag3_exponent", ctypes.c_int32), ("R0", ctypes.c_double),
                 ("h_slope", ctypes.c_double), ("diag3_factor", ctypes.c_double), ("dt_conn", ctypes.c_double),
                 ("m1", ctypes.c_double), ("m2", ctypes.c_double), ("separation", ctypes.c_double),
-                ("phase0", ctypes.c_double), ("inspiral", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("phase0", ctypes.c_double), ("inspiral", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("spin", ctypes.c_double)]
 
 
 def dyn_metric(spacetime=DYN_MINK_SPHERICAL, R0=0.0, h_slope=0.35, th_cutout=None, diag3_exponent=7, dt_conn=9.0e-6,
-               m1=0.5, m2=0.5, separation=20.0, phase0=0.0, inspiral=1):
+               m1=0.5, m2=0.5, separation=20.0, phase0=0.0, inspiral=1, spin=0.0):
     """The torus setup's coordinates (set_special_coord, init.torus.c:245-270:
     th_cutout = SMALL pi, diag3_factor = 1 - 2 th_cutout/pi - h_slope), the
-    driver's dt_conn (main.c:569) and, for DYN_PN_BINARY, the binary."""
+    driver's dt_conn (main.c:569), for DYN_PN_BINARY the binary and for
+    DYN_KS_SPHERICAL the spin."""
     import math
     if th_cutout is None:
         th_cutout = 1e-15 * math.pi
@@ -78,6 +81,7 @@ def dyn_metric(spacetime=DYN_MINK_SPHERICAL, R0=0.0, h_slope=0.35, th_cutout=Non
     m.diag3_factor = 1. - 2 * th_cutout / math.pi - h_slope
     m.dt_conn = dt_conn
     m.m1, m.m2, m.separation, m.phase0, m.inspiral = m1, m2, separation, phase0, inspiral
+    m.spin = spin
     return m
 
 

@@ -32,6 +32,7 @@ void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 cudaError_t prepare_kernels();
 void launch_geom_levels(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
+void launch_conn_broadcast(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *rows);
 void launch_totals(const GridDev &G, const LaunchCfg &L, cudaStream_t s, double *part, double *out);
 void launch_ref_to_planes(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *ref, int NT1, int NT2,
                           double *out);
@@ -800,9 +801,13 @@ extern "C" int hg_step(hg_handle *h, int32_t nsteps, double *t, double *dt)
 
 static int dyn_from_abi(const hg_dyn_metric *m, hg::DynMetric &dm)
 {
-  if (!m || (m->spacetime != HG_DYN_MINK_SPHERICAL && m->spacetime != HG_DYN_PN_BINARY) || m->diag3_exponent < 3 ||
-      !(m->dt_conn > 0.))
+  if (!m ||
+      (m->spacetime != HG_DYN_MINK_SPHERICAL && m->spacetime != HG_DYN_PN_BINARY &&
+       m->spacetime != HG_DYN_KS_SPHERICAL) ||
+      m->diag3_exponent < 3 || !(m->dt_conn > 0.))
     return HG_ERR_BADARG;
+  if (m->spacetime == HG_DYN_KS_SPHERICAL && !(fabs(m->spin) < 1.)) return HG_ERR_BADARG;
+  dm.spin = m->spin;
   if (m->spacetime == HG_DYN_PN_BINARY &&
       (!(m->m1 > 0.) || !(m->m2 > 0.) || !(m->separation > 0.) || (m->inspiral != 0 && m->inspiral != 1)))
     return HG_ERR_BADARG;
@@ -832,6 +837,30 @@ extern "C" int hg_set_dynamic_metric(hg_handle *h, const hg_dyn_metric *m)
     Gh.ctab = tab.data();
     hg::dyn_coord_tables(Gh, tab.data());
     HG_CK(copy_sync(h, h->G.ctab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+  }
+  if (h->G.dyn.spacetime == HG_DYN_KS_SPHERICAL) {
+    // the static analytic connection of the Kerr-Schild test spacetime
+    // (metric.c:3555-3558), the same in every phi layer: rows per (i, j),
+    // spread over k on the device
+    const hg::DynMetric &dm = h->G.dyn;
+    const int n1 = h->G.N[0], n2 = h->G.N[1];
+    std::vector<double> rows((size_t)64 * n1 * n2);
+    hg::ks_conn_rows(dm.spin, dm.R0, dm.h_slope, dm.diag3_factor, dm.diag3_exponent, h->d.startx, h->d.dx, n1, n2,
+                     rows.data());
+    void *drows = nullptr;  // set-up-time staging of the rows, freed below
+    if (cudaMalloc(&drows, sizeof(double) * rows.size()) != cudaSuccess) {
+      cudaGetLastError();
+      return HG_ERR_NOMEM;
+    }
+    cudaError_t e = cudaMemcpyAsync(drows, rows.data(), sizeof(double) * rows.size(), cudaMemcpyHostToDevice,
+                                    h->stream);
+    if (e == cudaSuccess) {
+      hg::launch_conn_broadcast(h->G, h->L, h->stream, (const double *)drows);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(drows);
+    HG_CK(e);
   }
   const int lev[3] = {0, 1, 2};  // n_beg, n_mid, n_end (init_general_metric, metric.c:3676-3679)
   HG_CK(copy_sync(h, sc_field(h->G, offsetof(hg::DevScalars, lev)), lev, sizeof(lev), cudaMemcpyHostToDevice));

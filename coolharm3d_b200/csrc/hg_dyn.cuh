@@ -156,6 +156,47 @@ HG_DYN_HD void dyn_gcon_sth(const double *x, double t2, double gcon[4][4])
 
 HG_DYN_HD double dyn_gdet_sth(const double *x, double t1) { return x[1] * x[1] * fabs(t1); }
 
+// Kerr-Schild, M = 1, spin a, from cos/sin th: ks_gcov_func, ks_gcon_func
+// (metric.c:1168-1250) and ks_gdet_func = bl_gdet_func (metric.c:523-540,
+// 1905-1910), in their operation order
+HG_DYN_HD void dyn_ks(double r, double cth, double sth, double a, double gcov[4][4], double gcon[4][4],
+                      double *gdet)
+{
+  const double M = 1., asq = a * a;
+#pragma unroll
+  for (int p = 0; p < 4; p++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) gcov[p][q] = gcon[p][q] = 0.;
+  {
+    const double t2 = r * r, t3 = asq, t5 = cth * cth, t7 = t2 + t3 * t5, t9 = M * r / t7, t10 = 2.0 * t9;
+    const double t13 = sth * sth;
+    gcov[0][0] = t10 - 1.0;
+    gcov[0][1] = t10;
+    gcov[0][3] = -2.0 * t9 * a * t13;
+    gcov[1][0] = t10;
+    gcov[1][1] = 1.0 + t10;
+    gcov[1][3] = -a * gcov[1][1] * t13;
+    gcov[2][2] = t7;
+    gcov[3][0] = gcov[0][3];
+    gcov[3][1] = gcov[1][3];
+    gcov[3][3] = t13 * (t2 + t3 * (1.0 + 2.0 * t9 * t13));
+  }
+  {
+    const double t1 = M * r, t2 = r * r, t3 = asq, t5 = cth * cth, t8 = 1 / (t2 + t3 * t5), t10 = 2.0 * t1 * t8;
+    gcon[0][0] = -1.0 - t10;
+    gcon[0][1] = t10;
+    gcon[1][0] = t10;
+    gcon[1][1] = (t2 - 2.0 * t1 + t3) * t8;
+    gcon[1][3] = a * t8;
+    gcon[2][2] = t8;
+    gcon[3][1] = gcon[1][3];
+    const double t14 = sth * sth;
+    gcon[3][3] = t8 / t14;
+  }
+  const double cos_2th = (cth - sth) * (cth + sth), r2 = r * r;
+  *gdet = r2 * fabs(sth) * (1. + 0.5 * (asq / r2) * (1. + cos_2th));
+}
+
 // The coordinates of a position from the tables: x (t, r, th, phi), the
 // diagonal Jacobian entries, sin/cos th, and dyn_coords' inverse and
 // determinant formed from them as dyn_coords forms them.
@@ -361,9 +402,13 @@ HG_DYN_HD void dyn_geom(const GridDev &G, int pos, int i, int j, int k, double t
     return;
   } else {
   double gc[4][4], gn[4][4];
-  dyn_gcov_sth(q.x, q.sth, gc);
-  dyn_gcon_sth(q.x, q.sth, gn);
-  g.g = dyn_gdet_sth(q.x, q.sth);
+  if (G.dyn.spacetime == HG_DYN_KS_SPHERICAL) {
+    dyn_ks(q.x[1], q.cth, q.sth, G.dyn.spin, gc, gn, &g.g);
+  } else {
+    dyn_gcov_sth(q.x, q.sth, gc);
+    dyn_gcon_sth(q.x, q.sth, gn);
+    g.g = dyn_gdet_sth(q.x, q.sth);
+  }
   // The sums of transform_rank2cov2/con2 in their order, leaving out the
   // terms whose Jacobian factor is exactly zero (most of them: COORD_DIAGONAL3
   // couples only r-x1 and th-x2); adding those zero products changes no sum.

@@ -196,6 +196,24 @@ void nt_u2(double a, double r, double &ut2, double &up2)
 
 }  // namespace
 
+namespace hg {
+// The Kerr-Schild connection of the physical zones (i, j) of a
+// COORD_DIAGONAL3 grid, rows (j + n2 i) of 64: the static connection of the
+// dynamic path's Kerr-Schild test spacetime (ks_conn_func at CENT,
+// metric.c:3555-3558), by the complex-step derivatives above.
+void ks_conn_rows(double a, double R0, double h_slope, double diag3_factor, int diag3_exponent, const double *startx,
+                  const double *dx, int n1, int n2, double *out)
+{
+  const KSParams P = {a, R0, h_slope, diag3_factor, diag3_exponent};
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < n2; j++) {
+      const double x1 = startx[1] + (i + HG_NG + 0.5) * dx[1];
+      const double x2 = seesaw01(startx[2] + (j + HG_NG + 0.5) * dx[2]);
+      conn_at(P, x1, x2, out + 64L * (j + (long)n2 * i));
+    }
+}
+}  // namespace hg
+
 extern "C" int hg_build_geometry_ks_mks(const hg_grid_desc *d, double a, double R0, double h_slope,
                                         double diag3_factor, int32_t diag3_exponent, double h_o_r, double *geom,
                                         double *conn, double *cell6, double *rface, double *cool_omega,

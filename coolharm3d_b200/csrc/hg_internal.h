@@ -52,6 +52,7 @@ struct DynMetric {
   double dt_conn;      // half-width of the connection's time difference (main.c:569)
   double m1, m2, sep, phase0;  // HG_DYN_PN_BINARY: the binary
   int inspiral;
+  double spin;                 // HG_DYN_KS_SPHERICAL: a (M = 1)
 };
 
 // Device-resident scalars of one grid (t, dx[0], reductions, failure flags).
@@ -175,5 +176,9 @@ __host__ __device__ inline void unpack_ijk(unsigned long long v, int &i, int &j,
   j = (int)((v >> 21) & 0x1FFFFF);
   k = (int)((v >> 42) & 0x1FFFFF);
 }
+
+// hg_geometry.cu: the Kerr-Schild connection rows of a COORD_DIAGONAL3 grid
+void ks_conn_rows(double a, double R0, double h_slope, double diag3_factor, int diag3_exponent, const double *startx,
+                  const double *dx, int n1, int n2, double *out);
 
 }  // namespace hg

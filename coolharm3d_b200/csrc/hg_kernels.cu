@@ -1493,7 +1493,7 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
   k_begin<<<1, 1, 0, s>>>(G.sc);
   // set_general_conn(t) before the predictor, set_general_conn(t + dx[0]/2)
   // before the corrector (step_ch.c:79-83, 128-133), from ncurr's level
-  if (G.mdim == 3) {
+  if (G.mdim == 3 && G.dyn.spacetime != HG_DYN_KS_SPHERICAL) {  // Kerr-Schild: static connection
     mark(R, KC_GEOM, s);
     k_conn_dyn<<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, 0.5 * sub);
   }
@@ -1853,6 +1853,25 @@ void launch_step(const GridDev &G, const LaunchCfg &L, cudaStream_t s, EventRec 
     launch_geom_level(G, L, s, 2, 1.0);
   }
   mark(R, KC_END, s);
+}
+
+// conn3 of the physical zones from rows (j + N1 i) of 64 that do not depend
+// on k (a static axisymmetric connection)
+__global__ void k_conn_broadcast(GridDev G, const double *rows)
+{
+  const unsigned N0 = G.N[0], N1 = G.N[1];
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < (unsigned)G.capacity; e += gridDim.x * blockDim.x) {
+    const unsigned q = e / N0;
+    const int ip = (int)(e - q * N0), jp = (int)(q % N1), kp = (int)(q / N1);
+    const long o = off3(G, HG_NGH + ip, HG_NGH + jp, HG_NGH + kp);
+    const double *r = rows + 64L * (jp + (long)N1 * ip);
+    for (int c = 0; c < 64; c++) G.conn3[c * G.S + o] = r[c];
+  }
+}
+
+void launch_conn_broadcast(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *rows)
+{
+  k_conn_broadcast<<<L.grid_upd, HG_BLK, 0, s>>>(G, rows);
 }
 
 // all three time levels at t (init_general_metric, metric.c:3664-3690)

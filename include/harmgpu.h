@@ -112,10 +112,13 @@ int hg_set_cooling_tables(hg_handle *h, const double *omega, const double *t_tar
  * gcov and the time difference of gcov over +-dt_conn (set_general_conn,
  * metric.c:3507-3648, conn.h).  The spacetime and its COORD_DIAGONAL3
  * coordinates (coord.c:270-276, set_special_coord of the setup) are
- * described here.  Spacetimes: HG_DYN_MINK_SPHERICAL, the reference's
- * METRIC_DYNAMIC_MINK_SPHERICAL test spacetime (options.h:90), and
- * HG_DYN_PN_BINARY below.  Every direction must be resolved (N > 1); FP64
+ * described here.  Spacetimes: HG_DYN_MINK_SPHERICAL and HG_DYN_KS_SPHERICAL,
+ * the reference's METRIC_DYNAMIC_MINK_SPHERICAL and _KS_SPHERICAL test
+ * spacetimes (options.h:88-90; Kerr-Schild takes the static analytic
+ * connection, as the reference does, metric.c:3555-3558, in place of the
+ * finite differences), and HG_DYN_PN_BINARY below.  Every direction must be resolved (N > 1); FP64
  * forms only. */
+#define HG_DYN_KS_SPHERICAL 0   /* METRIC_DYNAMIC_KS_SPHERICAL (options.h:88): Kerr-Schild, M = 1, spin a */
 #define HG_DYN_MINK_SPHERICAL 2
 /* HG_DYN_PN_BINARY: two point masses m1, m2 on a quasi-circular orbit in the
  * equatorial plane, in the first post-Newtonian harmonic-gauge metric
@@ -138,6 +141,8 @@ typedef struct hg_dyn_metric {
   double phase0;                /* orbital phase at t = 0 */
   int32_t inspiral;             /* 1: quadrupole-formula inspiral; 0: circular orbit */
   int32_t reserved;
+  /* HG_DYN_KS_SPHERICAL only */
+  double spin;                  /* a, |a| < 1 */
 } hg_dyn_metric;
 int hg_set_dynamic_metric(hg_handle *h, const hg_dyn_metric *m);
 /* The struct of_geom (HG_NGEOM doubles, hg_set_geometry's order) of position

@@ -120,6 +120,15 @@ CONFIGS = {
                            METRIC_TYPE_CHOICE="(METRIC_GENERAL_DYNAMIC)",
                            METRIC_DYNAMIC_TYPE_CHOICE="(METRIC_DYNAMIC_MINK_SPHERICAL)", SET_TSHRINK="(1)"),
                       None),
+    # The same torus on the dynamic path with the reference's Kerr-Schild test
+    # spacetime (METRIC_DYNAMIC_KS_SPHERICAL, options.h:88): geometry of
+    # the three time levels from ks_gcov/gcon/gdet_func, the static analytic
+    # connection in place of the finite differences (metric.c:3555-3558).
+    "torus_dynks": ("init.torus.c",
+                    dict(USE_COOLING_FUNCTION="(1)", FLUX_TYPE_CHOICE="(FLUX_HLLE)",
+                         METRIC_TYPE_CHOICE="(METRIC_GENERAL_DYNAMIC)",
+                         METRIC_DYNAMIC_TYPE_CHOICE="(METRIC_DYNAMIC_KS_SPHERICAL)", SET_TSHRINK="(1)"),
+                    None),
     # The circumbinary-disk setup of the post-Newtonian binary runs
     # (init.nz_pn_bbh_disk.c: De Villiers-Hawley-Krolik disk with q = 1.58
     # around the binary's total mass M = 1 at separation 20M, inner edge 2(a+M),
@@ -182,8 +191,9 @@ CONFIGS = {
 }
 
 
-# the dynamic-metric torus takes the torus configuration's edits of init.torus.c and phys.c
+# the dynamic-metric tori take the torus configuration's edits of init.torus.c and phys.c
 CONFIGS["torus_dynmink"] = CONFIGS["torus_dynmink"][:2] + (CONFIGS["torus"][2],)
+CONFIGS["torus_dynks"] = CONFIGS["torus_dynks"][:2] + (CONFIGS["torus"][2],)
 
 
 def set_define(text, name, value):

@@ -58,6 +58,9 @@ CASES = [
     # connection by 4th-order differences every substep
     ("torus_dynmink_12x10x6_s1", "torus_dynmink", (12, 10, 6), 1, "load"),
     ("torus_dynmink_12x10x6_s3", "torus_dynmink", (12, 10, 6), 3, "load"),
+    # and with the Kerr-Schild test spacetime (static analytic connection)
+    ("torus_dynks_12x10x6_s1", "torus_dynks", (12, 10, 6), 1, "load"),
+    ("torus_dynks_12x10x6_s3", "torus_dynks", (12, 10, 6), 3, "load"),
     # the circumbinary disk of the post-Newtonian binary setup
     # (init.nz_pn_bbh_disk.c) on the same path, the Minkowski-spherical test
     # spacetime standing in for the PN one the reference does not ship

@@ -32,6 +32,7 @@ CONFIG_SWITCHES = {
     "field_loop": dict(recon=5, flux=1, ct_para=1, bc=1, metric_dim=0, ee=1, cooling=0, rescale=0),
     "torus_dynmink": dict(recon=5, flux=1, ct_para=1, bc=10, metric_dim=3, ee=1, cooling=1, rescale=1),
     "pnbbh_dynmink": dict(recon=5, flux=1, ct_para=1, bc=10, metric_dim=3, ee=1, cooling=1, rescale=1),
+    "torus_dynks": dict(recon=5, flux=1, ct_para=1, bc=10, metric_dim=3, ee=1, cooling=1, rescale=1),
 }
 CONFIG_HOR = 0.1  # h_o_r of the torus and disk builds' cooling function (both set to 0.1)
 
@@ -40,6 +41,7 @@ CONFIG_HOR = 0.1  # h_o_r of the torus and disk builds' cooling function (both s
 CONFIG_DYN = {
     "torus_dynmink": dict(R0=0.0, h_slope=0.35, diag3_exponent=7),
     "pnbbh_dynmink": dict(R0=0.0, h_slope=0.0729419909586, diag3_exponent=9),
+    "torus_dynks": dict(R0=0.0, h_slope=0.35, diag3_exponent=7, spacetime=0, spin=0.9),  # DYN_KS_SPHERICAL
 }
 
 

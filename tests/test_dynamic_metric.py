@@ -2,10 +2,11 @@
 METRIC_GENERAL_DYNAMIC) against the reference's own build of it.
 
 Fixtures (tests/golden/make_golden.py, reference configurations
-torus_dynmink and pnbbh_dynmink of oracle/build_ref.py): the magnetised
-torus setup (12x10x6 zones) and the post-Newtonian binary's circumbinary
-disk setup (16x12x8 zones, init.nz_pn_bbh_disk.c) on the dynamic path with
-the reference's Minkowski-spherical test spacetime, 1 and 3 steps from the
+torus_dynmink, torus_dynks and pnbbh_dynmink of oracle/build_ref.py): the
+magnetised torus setup (12x10x6 zones) on the dynamic path with the
+reference's Minkowski-spherical and Kerr-Schild (a = 0.9) test spacetimes,
+and the post-Newtonian binary's circumbinary disk setup (16x12x8 zones,
+init.nz_pn_bbh_disk.c) with the Minkowski one, 1 and 3 steps from the
 reference's own initial data.  The
 reference keeps the geometry of three time levels in 3D tables (METRIC_DIM
 3), rotates them every step and rebuilds the connection before every
@@ -81,6 +82,25 @@ def test_host_evaluation_matches_reference_tables(name):
                     g = hg.dyn_geometry(d, m, pos, i, j, k, f["t0"])
                     r = ref[k + T[2] * (j + T[1] * (i + T[0] * pos))]
                     assert np.array_equal(g, r), (pos, i, j, k)
+
+
+def test_kerr_schild_connection_is_the_references():
+    """The Kerr-Schild test spacetime takes the static analytic connection
+    (ks_conn_func at CENT, metric.c:3555-3558); the engine's rows (the
+    complex-step derivatives of the static builder) agree with the
+    reference's closed form to 1e-14 of its largest entry, in every phi
+    layer."""
+    name = [n for n in NAMES if n.startswith("torus_dynks")][0]
+    f = fixtures.load(name)
+    n = f["n"]
+    d = hg.make_desc(n, f["gam"], f["cour"], f["dx"], f["startx"], f["grid_length"], metric_dim=2, cooling=1,
+                     rescale_r=1, bc=hg.BC_SPHERICAL_OUTFLOW3)
+    kw = ht.CONFIG_DYN["torus_dynks"]
+    t = hg.ks_mks_tables(d, a=kw["spin"], R0=kw["R0"], h_slope=kw["h_slope"], diag3_exponent=kw["diag3_exponent"])
+    rows = t["conn"].reshape(n[0], n[1], 64)
+    ref = f["conn"].reshape(n[0], n[1], n[2], 64)
+    for k in range(n[2]):
+        assert np.abs(rows - ref[:, :, k]).max() < 1e-14 * np.abs(ref).max(), k
 
 
 def test_init_refuses_unsupported_dynamic_grids():
