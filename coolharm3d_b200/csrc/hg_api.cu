@@ -166,7 +166,7 @@ static int validate(const hg_grid_desc *d)
   if (d->bc_type == 10 && (d->n1 == 1 || d->n2 == 1)) return HG_ERR_BADARG;
   if (d->metric_dim != 0 && d->metric_dim != 2 && d->metric_dim != 3) return HG_ERR_BADARG;
   // metric_dim 3 (time-dependent metric): every direction resolved, FP64 forms
-  if (d->metric_dim == 3 && (d->n1 == 1 || d->n2 == 1 || d->n3 == 1 || d->precision == HG_PREC_MIXED))
+  if (d->metric_dim == 3 && (d->n1 == 1 || d->n2 == 1 || d->n3 == 1))
     return HG_ERR_BADARG;
   if (d->cooling != 0 && d->cooling != 1) return HG_ERR_BADARG;
   if (d->precision != HG_PREC_FP64 && d->precision != HG_PREC_MIXED && d->precision != HG_PREC_FP64_FMA)
@@ -269,6 +269,8 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     if (G.prec == HG_PREC_MIXED) {
       ALLOC(G.p32, sizeof(float) * HG_NPR * G.S);
       if (G.mdim == 2) ALLOC(G.geomF, sizeof(float) * HG_GF * G.gS);
+      if (G.mdim == 3)
+        for (int l = 0; l < 3; l++) ALLOC(G.geomF3[l], sizeof(float) * HG_GF * 3 * G.S);
       if (G.rescale) ALLOC(G.rsc32, sizeof(float) * 12 * G.T[0]);
     }
     if (G.cooling) ALLOC(G.cool, sizeof(double) * 2 * G.T[0]);
@@ -715,7 +717,7 @@ extern "C" int hg_set_time(hg_handle *h, double t, double dt)
 static int refresh_levels(hg_handle *h)
 {
   if (h->G.mdim != 3 || !h->levels_stale) return HG_OK;
-  if (h->G.prec == HG_PREC_FP64_FMA) hg_fma::launch_geom_levels(h->G, h->L, h->stream);
+  if (fma_kernels(h->G)) hg_fma::launch_geom_levels(h->G, h->L, h->stream);  // the build the steps use
   else hg::launch_geom_levels(h->G, h->L, h->stream);
   HG_CK(cudaGetLastError());
   h->levels_stale = false;
@@ -1410,6 +1412,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   if (d->precision == HG_PREC_MIXED) {
     b += 4ull * HG_NPR * S;
     if (d->metric_dim == 2) b += 4ull * HG_GF * gS;
+    if (d->metric_dim == 3) b += 3ull * 4 * HG_GF * 3 * S;  // FP32 face geometry of the three levels
     if (d->rescale_r) b += 4ull * 12 * T[0];
   }
   b += 8ull * 148 * 8;                        // per-block partials

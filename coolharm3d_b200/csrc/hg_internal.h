@@ -122,6 +122,10 @@ struct GridDev {
   // th, dth/dx2, sin th, cos th, sin phi, cos phi), filled on the host with
   // the platform's libm (dyn_coord_tables, hg_dyn.cuh)
   double *ctab;
+  // metric_dim 3, mixed form: per level the FP32 face geometry of FACE1..3
+  // (HG_GF planes of 3*S floats, index d*S + zone offset), written by
+  // k_geom_level beside geomL
+  float *geomF3[3];
 };
 
 // metric_dim 3 level tables: the geometry the engine evaluates is symmetric

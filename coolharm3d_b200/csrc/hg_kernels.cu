@@ -45,7 +45,7 @@
 namespace hg {
 // the FP32 flux kernels of the mixed form (hg_mixed.cu)
 void launch_flux_f32(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d, const int *lo, const int *n,
-                     unsigned int mult);
+                     unsigned int mult, int slot);
 void launch_to_f32(const GridDev &G, int grid, cudaStream_t s, const double *src);
 }  // namespace hg
 
@@ -1255,6 +1255,23 @@ __global__ void __launch_bounds__(HG_BLK) k_geom_level(GridDev G, int slot, doub
     w[HG_DP_ALPHA * s] = g.alpha;
     for (int a = 0; a < 3; a++) w[(HG_DP_BETA + a) * s] = g.beta[a];
     w[HG_DP_NCON0 * s] = g.ncon[0];
+    if (G.geomF3[0] && pos < 3) {  // the mixed form's FP32 face geometry (hg_set_geometry's planes)
+      const int L = G.sc->lev[slot];
+      float *f = (L == 0 ? G.geomF3[0] : L == 1 ? G.geomF3[1] : G.geomF3[2]) + e;
+      const long fs = 3 * (long)G.S;
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) f[(a * 4 + b) * fs] = (float)g.gcov[a][b];
+      f[16 * fs] = (float)g.gcon[0][0];
+      for (int jj = 1; jj <= 3; jj++) {
+        f[(16 + jj) * fs] = (float)g.gcon[0][jj];
+        f[(19 + jj) * fs] = (float)g.gcon[jj][jj];
+      }
+      f[23 * fs] = (float)g.ncon[0];
+      for (int a = 0; a < 3; a++) f[(24 + a) * fs] = (float)g.beta[a];
+      f[27 * fs] = (float)g.g;
+    }
   }
 }
 
@@ -1458,7 +1475,7 @@ static void launch_flux_dir(const GridDev &G, const LaunchCfg &L, cudaStream_t s
     }
     mark(R, KC_FLUX, s);
     if (G.prec == HG_PREC_MIXED) {
-      launch_flux_f32(G, L, s, d, lo, n, mult);  // reads G.p32, filled from ph
+      launch_flux_f32(G, L, s, d, lo, n, mult, slot);  // reads G.p32, filled from ph
       return;
     }
 #define HG_FLUX(RSV, MD, DD) \

@@ -41,7 +41,7 @@ struct GeomF {
 // metric_dim 0: the one geometry of the grid, rounded; metric_dim 2: the
 // FP32 table built by hg_set_geometry (HG_GF planes, see hg_internal.h)
 template <int MDIM>
-__device__ __forceinline__ void geom_f32(const GridDev &G, int d, int i, int j, GeomF &f)
+__device__ __forceinline__ void geom_f32(const GridDev &G, int d, int i, int j, GeomF &f, int k = 0, int slot = 0)
 {
   const int js = d + 1;
   if (MDIM == 0) {
@@ -59,9 +59,17 @@ __device__ __forceinline__ void geom_f32(const GridDev &G, int d, int i, int j, 
     f.beta[2] = (float)g.beta[2];
     f.g = (float)g.g;
   } else {
-    const int ii = G.deg[0] ? 0 : i, jj = G.deg[1] ? 0 : j;
-    const float *t = G.geomF + ((long)d * G.T[1] + jj) * G.T[0] + ii;
-    const long s = G.gS;
+    const float *t;
+    long s;
+    if (MDIM == 3) {  // the level's table, written by k_geom_level
+      const int L = G.sc->lev[slot];
+      t = (L == 0 ? G.geomF3[0] : L == 1 ? G.geomF3[1] : G.geomF3[2]) + (long)d * G.S + off3(G, i, j, k);
+      s = 3 * (long)G.S;
+    } else {
+      const int ii = G.deg[0] ? 0 : i, jj = G.deg[1] ? 0 : j;
+      t = G.geomF + ((long)d * G.T[1] + jj) * G.T[0] + ii;
+      s = G.gS;
+    }
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -155,7 +163,7 @@ void launch_mirror_check(const GridDev &G, int grid, cudaStream_t s, const doubl
 template <bool RS, int MDIM, int d>
 __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_f32(const __grid_constant__ GridDev G, int lo0,
                                                                     int lo1, int lo2, int n0, int n1, int n2,
-                                                                    unsigned int mult)
+                                                                    unsigned int mult, int slot)
 {
   const unsigned total = (unsigned)n0 * n1 * n2;  // < 2^31 (hg_init)
   const int dim = d + 1;
@@ -170,7 +178,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_f32(const __gri
     float pl[HG_NPR], pr[HG_NPR];
     face_prims_f32<RS>(G, d, i, j, k, pl, pr);
     GeomF g;
-    geom_f32<MDIM>(G, d, i, j, g);
+    geom_f32<MDIM>(G, d, i, j, g, k, slot);
     StateT<float> ql, qr;
     if (get_state(pl, g, gam, ql)) book_face(G, i, j, k, mult);
     if (get_state(pr, g, gam, qr)) book_face(G, i, j, k, mult);
@@ -263,12 +271,12 @@ __device__ __forceinline__ void strip_recon_f32(const GridDev &G, const float *_
 // HLL/LF flux of one face from FP32 states; returns ctop
 template <int MDIM, int d>
 __device__ __forceinline__ float face_flux_f32(const GridDev &G, const float *pl, const float *pr, int i, int j, int k,
-                                               unsigned int mult, long o)
+                                               unsigned int mult, long o, int slot)
 {
   const int dim = d + 1;
   const float gam = (float)G.gam;
   GeomF g;
-  geom_f32<MDIM>(G, d, i, j, g);
+  geom_f32<MDIM>(G, d, i, j, g, k, slot);
   StateT<float> ql, qr;
   if (get_state(pl, g, gam, ql)) book_face(G, i, j, k, mult);
   if (get_state(pr, g, gam, qr)) book_face(G, i, j, k, mult);
@@ -303,7 +311,7 @@ __device__ __forceinline__ float face_flux_f32(const GridDev &G, const float *pl
 template <bool RS, int MDIM, int d, int NF>
 __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const __grid_constant__ GridDev G, int lo0,
                                                                           int lo1, int lo2, int n0, int n1, int n2,
-                                                                          unsigned int mult)
+                                                                          unsigned int mult, int slot)
 {
   __shared__ float sm[16 * NF * HG_BLK];
   const int tx = threadIdx.x;
@@ -344,7 +352,7 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const
         pr[l] = sm[(2 * NF * l + NF + s) * HG_BLK + tx];
       }
       const long o = o0 + s * st;
-      const float ctop = face_flux_f32<MDIM, d>(G, pl, pr, i, j, k, mult, o);
+      const float ctop = face_flux_f32<MDIM, d>(G, pl, pr, i, j, k, mult, o, slot);
       if (d == 0 && G.bc == 10) {  // fix_flux(), bounds.c:2263-2275
         double *fr = G.F[0] + RHO * G.S + o;
         if (i == HG_NGH && *fr > 0) *fr = 0.;
@@ -359,10 +367,11 @@ __global__ void __launch_bounds__(HG_BLK, HG_FLUX32_MINB) k_flux_strip_f32(const
 
 template <bool RS, int MDIM, int d>
 static void launch_strip32(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const int *lo, const int *n,
-                           unsigned int mult)
+                           unsigned int mult, int slot)
 {
 #define HG_S32N(NF) \
-  k_flux_strip_f32<RS, MDIM, d, NF><<<L.grid_flux32, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
+  k_flux_strip_f32<RS, MDIM, d, NF><<<L.grid_flux32, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult, \
+                                                                     slot)
   if (L.strip_nf <= 1) HG_S32N(1);
   else if (L.strip_nf == 2) HG_S32N(2);
   else HG_S32N(3);
@@ -370,18 +379,21 @@ static void launch_strip32(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
 }
 
 void launch_flux_f32(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int d, const int *lo, const int *n,
-                     unsigned int mult)
+                     unsigned int mult, int slot)
 {
   const int grid = L.grid_flux32;
 #define HG_F32(RSV, MD, DD) \
-  k_flux_f32<RSV, MD, DD><<<grid, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult)
+  k_flux_f32<RSV, MD, DD><<<grid, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2], mult, slot)
 #define HG_F32_D(RSV, MD) \
-  if (d == 0) { if (G.deg[0] || !L.strip_x1) HG_F32(RSV, MD, 0); else launch_strip32<RSV, MD, 0>(G, L, s, lo, n, mult); } \
-  else if (d == 1) { if (G.deg[1]) HG_F32(RSV, MD, 1); else launch_strip32<RSV, MD, 1>(G, L, s, lo, n, mult); } \
-  else { if (G.deg[2]) HG_F32(RSV, MD, 2); else launch_strip32<RSV, MD, 2>(G, L, s, lo, n, mult); }
+  if (d == 0) { if (G.deg[0] || !L.strip_x1) HG_F32(RSV, MD, 0); else launch_strip32<RSV, MD, 0>(G, L, s, lo, n, mult, slot); } \
+  else if (d == 1) { if (G.deg[1]) HG_F32(RSV, MD, 1); else launch_strip32<RSV, MD, 1>(G, L, s, lo, n, mult, slot); } \
+  else { if (G.deg[2]) HG_F32(RSV, MD, 2); else launch_strip32<RSV, MD, 2>(G, L, s, lo, n, mult, slot); }
   if (G.mdim == 0) {
     if (G.rescale) { HG_F32_D(true, 0) }
     else { HG_F32_D(false, 0) }
+  } else if (G.mdim == 3) {
+    if (G.rescale) { HG_F32_D(true, 3) }
+    else { HG_F32_D(false, 3) }
   } else {
     if (G.rescale) { HG_F32_D(true, 2) }
     else { HG_F32_D(false, 2) }

@@ -107,7 +107,7 @@ def test_init_refuses_unsupported_dynamic_grids():
     f = fixtures.load(NAMES[0])
     lib = hg.load_library()
     import ctypes
-    for kw in (dict(n=(12, 10, 1)), dict(precision=hg.PREC_MIXED)):
+    for kw in (dict(n=(12, 10, 1)), dict(n=(1, 10, 6))):
         n = kw.get("n", f["n"])
         d = hg.make_desc(n, f["gam"], f["cour"], f["dx"], f["startx"], f["grid_length"], metric_dim=3, bc=10,
                          precision=kw.get("precision", hg.PREC_FP64))
