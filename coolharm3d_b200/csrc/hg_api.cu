@@ -262,7 +262,7 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     if (G.mdim == 3) {  // three time levels of 42 planes of 5 positions, the substep's connection
       G.gS3 = (long)HG_DYN_NPOS * G.S;
       for (int l = 0; l < 3; l++) ALLOC(G.geomL[l], sizeof(double) * HG_DYN_PLANES * G.gS3);
-      ALLOC(G.conn3, sizeof(double) * 64 * G.S);
+      ALLOC(G.conn3, sizeof(double) * HG_CONN3_PLANES * G.S);
       ALLOC(G.ctab, sizeof(double) * hg::dyn_tab_layout(G.T).total);
     }
     if (G.rescale) ALLOC(G.rsc, sizeof(double) * 12 * G.T[0]);
@@ -1406,7 +1406,7 @@ extern "C" int hg_grid_bytes(const hg_grid_desc *d, uint64_t *bytes)
   b += sizeof(hg::DevScalars) + 8ull * cap * (2 + HG_NPR);  // scalars, queue, flagged list
   if (d->use_entropy_eq) b += 8ull * 6 * cap;                 // entropy face fluxes of the queue
   if (d->metric_dim == 2) b += 8ull * 42 * gS + 8ull * 64 * T[0] * T[1];
-  if (d->metric_dim == 3) b += 3ull * 8 * HG_DYN_PLANES * HG_DYN_NPOS * S + 8ull * 64 * S + 8ull * (4 * T[0] + 8 * T[1] + 4 * T[2]);  // coordinate tables
+  if (d->metric_dim == 3) b += 3ull * 8 * HG_DYN_PLANES * HG_DYN_NPOS * S + 8ull * HG_CONN3_PLANES * S + 8ull * (4 * T[0] + 8 * T[1] + 4 * T[2]);  // coordinate tables
   if (d->rescale_r) b += 8ull * 12 * T[0];
   if (d->cooling) b += 8ull * 2 * T[0];
   if (d->precision == HG_PREC_MIXED) {

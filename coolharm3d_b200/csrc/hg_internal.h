@@ -112,8 +112,8 @@ struct GridDev {
   Geom g0;                   // metric_dim 0 geometry
   // metric_dim 3: three time levels of geometry, each HG_DYN_PLANES planes
   // of gS3 = 5*S doubles (index pos*S + zone offset), filled by
-  // k_geom_level; the connection of the current substep, 64 planes of S
-  // (k_conn_dyn)
+  // k_geom_level; the connection of the current substep, HG_CONN3_PLANES
+  // planes of S (k_conn_dyn)
   double *geomL[3];
   long gS3;
   double *conn3;
@@ -149,6 +149,11 @@ __host__ __device__ __forceinline__ int dyn_sym(int a, int b)
   const int lo = a < b ? a : b, hi = a < b ? b : a;
   return lo * 4 - (lo * (lo - 1)) / 2 + (hi - lo);  // (0,0)..(0,3) 0..3, (1,1)..(1,3) 4..6, (2,2) 7, (2,3) 8, (3,3) 9
 }
+
+// metric_dim 3 connection: conn[a][b][c] = conn[a][c][b] to the bit (the
+// two swapped terms of DGCOV_TO_CONN add in the other order), so conn3
+// keeps the 40 entries b <= c, plane a*10 + dyn_sym(b, c).
+#define HG_CONN3_PLANES 40
 
 // Fixed grid sizes of the step's kernels (grid-stride loops).
 struct LaunchCfg {

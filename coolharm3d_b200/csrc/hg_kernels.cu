@@ -463,10 +463,10 @@ __device__ __forceinline__ int source_terms(const GridDev &G, const double *ph, 
       for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) {
-          dU[U1] += mhd[a][b] * G.conn3[((b * 4 + 1) * 4 + a) * cS + co];
-          dU[U2] += mhd[a][b] * G.conn3[((b * 4 + 2) * 4 + a) * cS + co];
-          dU[UU] += mhd[a][b] * G.conn3[((b * 4 + 0) * 4 + a) * cS + co];
-          dU[U3] += mhd[a][b] * G.conn3[((b * 4 + 3) * 4 + a) * cS + co];
+          dU[U1] += mhd[a][b] * G.conn3[(b * 10 + dyn_sym(1, a)) * cS + co];
+          dU[U2] += mhd[a][b] * G.conn3[(b * 10 + dyn_sym(2, a)) * cS + co];
+          dU[UU] += mhd[a][b] * G.conn3[(b * 10 + dyn_sym(0, a)) * cS + co];
+          dU[U3] += mhd[a][b] * G.conn3[(b * 10 + dyn_sym(3, a)) * cS + co];
         }
     } else {
       const long cS = (long)G.T[0] * G.T[1];
@@ -1298,8 +1298,11 @@ __device__ __forceinline__ double dyn_gcov_at(const GridDev &G, const double *lv
 // (conn.h:44-86, weights invdx/6 and 4 invdx/3), on a physical x2 boundary
 // the one-sided x2 stencils of conn_func_fd4_lo2 / _hi2 (metric.c:254-340,
 // weights metric.c:3526-3540) -- and DGCOV_TO_CONN (conn.h:25-37) with the
-// zone's gcon.  Written to conn3 in conn[a][b][c] order.
-__global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double tfac)
+// zone's gcon.  Written to conn3 as the 40 entries b <= c (HG_CONN3_PLANES).
+#ifndef HG_CONN_MINB
+#define HG_CONN_MINB 4
+#endif
+__global__ void __launch_bounds__(HG_BLK, HG_CONN_MINB) k_conn_dyn(GridDev G, int slot, double tfac)
 {
   const double *lv = dyn_level(G, slot);
   const double t = G.sc->t + tfac * G.sc->dt;
@@ -1372,12 +1375,12 @@ __global__ void __launch_bounds__(HG_BLK) k_conn_dyn(GridDev G, int slot, double
 #pragma unroll
       for (int b = 0; b < 4; b++)
 #pragma unroll
-        for (int cc = 0; cc < 4; cc++) {
+        for (int cc = b; cc < 4; cc++) {  // conn[a][cc][b] is the same double (HG_CONN3_PLANES)
           double v = 0.;
 #pragma unroll
           for (int l = 0; l < 4; l++)
             v += gcon[a][l] * (0.5 * (dg[dyn_sym(b, l)][cc] + dg[dyn_sym(cc, l)][b] - dg[dyn_sym(cc, b)][l]));
-          G.conn3[((a * 4 + b) * 4 + cc) * G.S + o] = v;
+          G.conn3[(a * 10 + dyn_sym(b, cc)) * G.S + o] = v;
         }
   }
 }
@@ -1882,7 +1885,9 @@ __global__ void k_conn_broadcast(GridDev G, const double *rows)
     const int ip = (int)(e - q * N0), jp = (int)(q % N1), kp = (int)(q / N1);
     const long o = off3(G, HG_NGH + ip, HG_NGH + jp, HG_NGH + kp);
     const double *r = rows + 64L * (jp + (long)N1 * ip);
-    for (int c = 0; c < 64; c++) G.conn3[c * G.S + o] = r[c];
+    for (int a = 0; a < 4; a++)
+      for (int b = 0; b < 4; b++)
+        for (int c = b; c < 4; c++) G.conn3[(a * 10 + dyn_sym(b, c)) * G.S + o] = r[(a * 4 + b) * 4 + c];
   }
 }
 
