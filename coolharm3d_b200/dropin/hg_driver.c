@@ -18,6 +18,10 @@
  * current: t, t_old, dx[0], dt_old, nfailtot and M_tot every step, p (and
  * pflag, p_gamma) whenever the host is about to read them.
  *
+ * METRIC_GENERAL_DYNAMIC (METRIC_DIM 3) with the Minkowski- or
+ * Kerr-Schild-spherical test spacetime is described to the library by
+ * hg_set_dynamic_metric(); the library evaluates its geometry itself.
+ *
  * USE_COOLING_FUNCTION 1 needs the h_o_r of cooling_func_hr_disk()
  * (phys.c:655, a constant local there): define HG_DROPIN_H_O_R to it. */
 #include "decs.h"
@@ -51,7 +55,7 @@ static void hg_check(int rc, const char *what)
  * geometry, coordinate data and primitives to the GPU */
 void hg_gpu_init(void)
 {
-  int i, j, k, l, a, b, c;
+  int i, j, k, l, ia, ib, ic; /* not a, b, c: a is the global spin */
   hg_grid_desc d;
   memset(&d, 0, sizeof(d));
   d.n1 = N1;
@@ -77,17 +81,41 @@ void hg_gpu_init(void)
   }
   hg_check(hg_init(&d, &gpu_grid), "hg_init");
 
+#if METRIC_DIM == 3
+  {
+    /* METRIC_GENERAL_DYNAMIC: the library evaluates the three time levels
+     * and the connection on the device; it takes the spacetime and the
+     * COORD_DIAGONAL3 parameters of set_special_coord() */
+    hg_dyn_metric m;
+    memset(&m, 0, sizeof(m));
+#if METRIC_DYNAMIC_TYPE_CHOICE == METRIC_DYNAMIC_MINK_SPHERICAL
+    m.spacetime = HG_DYN_MINK_SPHERICAL;
+#elif METRIC_DYNAMIC_TYPE_CHOICE == METRIC_DYNAMIC_KS_SPHERICAL
+    m.spacetime = HG_DYN_KS_SPHERICAL;
+    m.spin = a;
+#else
+#error "USE_GPU_STEP: this METRIC_DYNAMIC_TYPE_CHOICE has no spacetime in libharmgpu"
+#endif
+    m.R0 = R0;
+    m.h_slope = h_slope;
+    m.diag3_factor = diag3_factor;
+    m.diag3_exponent = diag3_exponent;
+    m.dt_conn = dt_conn;
+    hg_check(hg_set_dynamic_metric(gpu_grid, &m), "hg_set_dynamic_metric");
+  }
+#else
   /* geom_arr[0] is one allocation of N_GEOM structs of 42 doubles
    * (decomp.c:168); conn is a pointer tree with a separate 4-double leaf per
    * [l][a][b] (ALLOC_4D_ARRAY, decomp.c:171), gathered here into one array */
   double *cbuf = (double *)malloc(sizeof(double) * 64 * (N_CONN > 0 ? N_CONN : 1));
   if (!cbuf) fail(FAIL_BASIC, 0);
   for (l = 0; l < N_CONN; l++)
-    for (a = 0; a < NDIM; a++)
-      for (b = 0; b < NDIM; b++)
-        for (c = 0; c < NDIM; c++) cbuf[((l * NDIM + a) * NDIM + b) * NDIM + c] = conn[l][a][b][c];
+    for (ia = 0; ia < NDIM; ia++)
+      for (ib = 0; ib < NDIM; ib++)
+        for (ic = 0; ic < NDIM; ic++) cbuf[((l * NDIM + ia) * NDIM + ib) * NDIM + ic] = conn[l][ia][ib][ic];
   hg_check(hg_set_geometry(gpu_grid, (const double *)geom_arr[0], N_GEOM, cbuf, N_CONN), "hg_set_geometry");
   free(cbuf);
+#endif
 
   /* per-cell floors and coordinates at CENT (coord.c:3754-3800) */
   double *cell6 = (double *)malloc(sizeof(double) * 6 * N1TOT * N2TOT * N3TOT);

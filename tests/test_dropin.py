@@ -12,10 +12,15 @@ Two configurations staged by oracle/build_ref.py:
     final time 10000 -> 5e-3 (19 steps), and the setup's random
     perturbation of u switched off, because the reference seeds it from the
     wall clock (ranc.c:37-41) and the two programs must start alike.
+  * torus_dynmink and pnbbh_dynmink (the torus and the post-Newtonian
+    binary's circumbinary disk on the time-dependent metric path with the
+    Minkowski-spherical test spacetime: hg_set_dynamic_metric in place of
+    the geometry tables): final time 2e-3.
 These test-only edits go to both builds.  Both programs run the whole driver
 loop; the GPU program's restart files (restart_write(): the ASCII rdump the
 driver writes every n_restart steps and at the end) must be byte for byte
-the CPU program's, and its energy file (dump_ener every 10 steps: U and
+the CPU program's -- but for at most a few numbers within 1e-12, where
+glibc's pow() is misrounded and the engine's entropy-fix pow() is not -- and its energy file (dump_ener every 10 steps: U and
 boundary-flux integrals summed on the device, M_tot from the device) must
 agree to 1e-12 relative, per column group (the sums' order differs)."""
 import os
@@ -44,6 +49,13 @@ CASES = {
               [(r"GridLength\[0\] = 10000\. ;", "GridLength[0] = 5.e-3 ;"),
                (r"(?m)^  randfact = 4\.e-2;", "  randfact = 0.;")],
               ["-DHG_DROPIN_H_O_R=1.e-1"]),
+    "torus_dynmink": ((12, 10, 6), "init.torus.c",
+                      [(r"GridLength\[0\] = 10000\. ;", "GridLength[0] = 2.e-3 ;"),
+                       (r"(?m)^  randfact = 4\.e-2;", "  randfact = 0.;")],
+                      ["-DHG_DROPIN_H_O_R=1.e-1"]),
+    "pnbbh_dynmink": ((16, 12, 8), "init.nz_pn_bbh_disk.c",
+                      [(r"GridLength\[0\] = 10000\. ;", "GridLength[0] = 2.e-3 ;")],
+                      ["-DHG_DROPIN_H_O_R=1.e-1"]),
 }
 
 
@@ -119,7 +131,20 @@ def test_patched_driver_reproduces_cpu_run(cfg):
         dumps = sorted(p.name for p in rc.glob("rdump*"))
         assert dumps and dumps == sorted(p.name for p in rg.glob("rdump*"))
         for name in dumps:
-            assert (rc / name).read_bytes() == (rg / name).read_bytes(), name
+            a, b = (rc / name).read_bytes(), (rg / name).read_bytes()
+            if a != b:
+                # the one exception to byte identity: zones where glibc's pow()
+                # is misrounded and the engine's correctly rounded pow() of the
+                # entropy fix is not (tests/test_crpow.py): a few numbers
+                # differing in their last digits
+                ta, tb = a.split(), b.split()
+                assert len(ta) == len(tb), name
+                diff = [(x, y) for x, y in zip(ta, tb) if x != y]
+                assert len(diff) <= 4, (name, len(diff))
+                for x, y in diff:
+                    fx, fy = float(x), float(y)
+                    assert abs(fx - fy) <= 1e-12 * max(abs(fx), abs(fy)), (name, x, y)
+                print(cfg, name, "values differing by rounding:", len(diff))
         # the driver's step count and zone-cycles line (main.c:117)
         ns = [line for line in out_c.splitlines() if line.startswith("ns,ts")]
         assert ns and ns == [line for line in out_g.splitlines() if line.startswith("ns,ts")]
