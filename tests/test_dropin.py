@@ -12,10 +12,12 @@ Two configurations staged by oracle/build_ref.py:
     final time 10000 -> 5e-3 (19 steps), and the setup's random
     perturbation of u switched off, because the reference seeds it from the
     wall clock (ranc.c:37-41) and the two programs must start alike.
-  * torus_dynmink and pnbbh_dynmink (the torus and the post-Newtonian
-    binary's circumbinary disk on the time-dependent metric path with the
-    Minkowski-spherical test spacetime: hg_set_dynamic_metric in place of
-    the geometry tables): final time 2e-3.
+  * torus_dynmink, torus_dynks and pnbbh_dynmink (the torus and the
+    post-Newtonian binary's circumbinary disk on the time-dependent metric
+    path with the Minkowski-spherical, and the torus with the Kerr-Schild,
+    test spacetime: hg_set_dynamic_metric in place of the geometry tables):
+    final time 2e-3; the Kerr-Schild one is compared value by value
+    (RDUMP_RTOL), its connection not being the reference's to the bit.
 These test-only edits go to both builds.  Both programs run the whole driver
 loop; the GPU program's restart files (restart_write(): the ASCII rdump the
 driver writes every n_restart steps and at the end) must be byte for byte
@@ -53,10 +55,22 @@ CASES = {
                       [(r"GridLength\[0\] = 10000\. ;", "GridLength[0] = 2.e-3 ;"),
                        (r"(?m)^  randfact = 4\.e-2;", "  randfact = 0.;")],
                       ["-DHG_DROPIN_H_O_R=1.e-1"]),
+    "torus_dynks": ((12, 10, 6), "init.torus.c",
+                    [(r"GridLength\[0\] = 10000\. ;", "GridLength[0] = 2.e-3 ;"),
+                     (r"(?m)^  randfact = 4\.e-2;", "  randfact = 0.;")],
+                    ["-DHG_DROPIN_H_O_R=1.e-1"]),
     "pnbbh_dynmink": ((16, 12, 8), "init.nz_pn_bbh_disk.c",
                       [(r"GridLength\[0\] = 10000\. ;", "GridLength[0] = 2.e-3 ;")],
                       ["-DHG_DROPIN_H_O_R=1.e-1"]),
 }
+
+
+# configurations compared value by value instead of byte by byte: the
+# Kerr-Schild dynamic torus takes its static connection from the engine's
+# complex-step derivatives, within 1e-14 of the reference's closed form
+# (tests/test_dynamic_metric.py), not bit for bit; over the 16 steps the
+# difference grows to 1.3e-9 of a variable's largest magnitude (measured)
+RDUMP_RTOL = {"torus_dynks": 5e-9}
 
 
 def staged(cfg):
@@ -132,7 +146,21 @@ def test_patched_driver_reproduces_cpu_run(cfg):
         assert dumps and dumps == sorted(p.name for p in rg.glob("rdump*"))
         for name in dumps:
             a, b = (rc / name).read_bytes(), (rg / name).read_bytes()
-            if a != b:
+            if a != b and cfg in RDUMP_RTOL:
+                # header (t, sizes, nstep, ..., dx[0]) within 1e-12; the body,
+                # one line of 8 primitives per zone, per variable against
+                # that variable's largest magnitude
+                la, lb = a.decode().splitlines(), b.decode().splitlines()
+                assert len(la) == len(lb), name
+                np.testing.assert_allclose(np.array(lb[0].split(), float), np.array(la[0].split(), float),
+                                           rtol=1e-12)
+                pa = np.array([x.split() for x in la[1:]], float)
+                pb = np.array([x.split() for x in lb[1:]], float)
+                scale = np.abs(pa).max(0)
+                worst = (np.abs(pa - pb).max(0) / np.where(scale > 0, scale, 1.)).max()
+                print(cfg, name, "largest difference per variable scale:", worst)
+                assert worst <= RDUMP_RTOL[cfg], (name, worst)
+            elif a != b:
                 # the one exception to byte identity: zones where glibc's pow()
                 # is misrounded and the engine's correctly rounded pow() of the
                 # entropy fix is not (tests/test_crpow.py): a few numbers

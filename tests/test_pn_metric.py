@@ -172,3 +172,48 @@ def test_disk_runs_in_the_pn_metric():
     # the radial velocity the flow develops differs by far more than rounding
     # (measured: 1e-4 of itself after six steps, t ~ 1e-4)
     assert np.abs(a[inside][:, 2] - b[inside][:, 2]).max() > 1e-6 * np.abs(b[inside][:, 2]).max()
+
+
+def test_block_evaluation_is_the_pointwise_one():
+    """hg_dyn_geometry_block (whole i-planes on host threads) returns, per
+    zone, exactly hg_dyn_geometry's struct, for each spacetime."""
+    d = pnbbh.pnbbh_desc(N)
+    for m in (pnbbh.pnbbh_coords(), pn(inspiral=1), pnbbh.pnbbh_coords(spacetime=hg.DYN_KS_SPHERICAL, spin=0.5)):
+        blk = hg.dyn_geometry_block(d, m, 3, 2.5, 4, 3)
+        for (i, j, k) in [(4, 0, 0), (5, 7, 3), (6, 17, 13)]:
+            assert np.array_equal(blk[i - 4, j, k], hg.dyn_geometry(d, m, 3, i, j, k, 2.5)), (i, j, k)
+
+
+@pytest.mark.gpu
+def test_dynamic_grids_step_in_a_batch_as_alone():
+    """Grids on the time-dependent metric path (their levels rotate on the
+    device inside each member's graph) advance in a batch exactly as alone."""
+    ms = [pnbbh.pnbbh_coords(), pn(inspiral=1)]
+    p0 = None
+    engines = []
+    for m in ms:
+        e, d, t = engine(m)
+        e.set_cooling_tables(t["cool_omega"], t["cool_temp"])
+        if p0 is None:
+            p0, _ = pnbbh.set_disk(e, d, t, m)
+        else:
+            e.upload(p0)
+        e.set_time(0.0, d.dx[0])
+        engines.append(e)
+    b = hg.Batch(0, 4)
+    for e in engines:
+        b.add(e)
+    for _ in range(4):
+        b.step()
+    for e in engines:
+        b.remove(e)
+    b.close()
+    for m, e in zip(ms, engines):
+        a, d, t = engine(m)
+        a.set_cooling_tables(t["cool_omega"], t["cool_temp"])
+        a.upload(p0)
+        a.set_time(0.0, d.dx[0])
+        a.step(4)
+        assert np.array_equal(e.download(), a.download())
+        a.close()
+        e.close()
