@@ -106,3 +106,29 @@ def test_fma_multi_step_fixtures(name):
     assert e.fail_counts().tolist() == f["nfailtot"].tolist()
     assert d.max() <= (1e-7 if "stress" in name else L1_BAR)
     e.close()
+
+
+@pytest.mark.parametrize("name", fixtures.dynamic_names())
+def test_fma_on_the_dynamic_metric_path(name):
+    """metric_dim 3 in the FMA form: the time levels and the connection are
+    evaluated by the contracted build too.  Primitives within 1e-10 of each
+    variable's largest magnitude after one step (flags equal) and 1e-9 after
+    three.  Measured: 1e-12 .. 1e-15 on the Minkowski fixtures; 3.4e-11 in U1
+    on the Kerr-Schild one, whose connection already differs from the
+    reference's closed form by 1e-14."""
+    from test_dynamic_metric import desc_of, metric_of
+    f = fixtures.load(name)
+    e = hg.Engine(desc_of(f, hg.PREC_FP64_FMA))
+    e.set_dynamic_metric(metric_of(f))
+    e.set_cell_data(fixtures.cell6_of(f), f["rface"])
+    e.set_cooling_tables(f["cool_omega"], f["cool_temp"])
+    e.upload(f["p0"])
+    e.set_time(f["t0"], f["dt0"])
+    e.step(f["steps"])
+    n = f["n"]
+    d = normwise_rel(ht.interior(e.download(), n), ht.interior(f["p"], n))
+    print(name, d)
+    assert d.max() <= (1e-10 if f["steps"] == 1 else 1e-9)
+    if f["steps"] == 1:
+        assert np.array_equal(e.pflag(), f["pflag"])
+    e.close()
