@@ -549,11 +549,14 @@ __device__ __forceinline__ void update_zone(const GridDev &G, int i, int j, int 
 //                  (the Uc planes) and the per-block M_tot partials;
 //   k_update_c2p   the 2D Newton inversion of U, the queue for the rest of
 //                  recover_primitives(), floors and gamma ceiling -> p_f.
-// sub = 0 predictor (p_f = ph), 1 corrector (p_f = p).
-template <bool RS, int MDIM>
-__global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __grid_constant__ GridDev G, int sub,
+// sub = 0 predictor (p_f = ph), 1 corrector (p_f = p).  The conserved update
+// takes it as a template parameter: each substep's kernel holds only its own
+// source path (fewer registers, no spill at the 3-block cap).
+template <bool RS, int MDIM, int SUB>
+__global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __grid_constant__ GridDev G,
                                                                     double dtfac, const double *__restrict__ p_h)
 {
+  constexpr int sub = SUB;
   const unsigned N0 = G.N[0], N1 = G.N[1];
   const unsigned total = (unsigned)G.capacity;  // < 2^31 (hg_init)
   const double Dt = dtfac * G.sc->dt;
@@ -1529,8 +1532,9 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
     k_emf<<<L.grid_emf, HG_BLK, 0, s>>>(G, lo[0], lo[1], lo[2], n[0], n[1], n[2]);
   }
   mark(R, KC_UPDATE, s);
-#define HG_UPD(RSV, MD)                                                      \
-  k_update_cons<RSV, MD><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, dtfac, ph); \
+#define HG_UPD(RSV, MD)                                                                       \
+  if (sub == 0) k_update_cons<RSV, MD, 0><<<L.grid_upd, HG_BLK, 0, s>>>(G, dtfac, ph);        \
+  else k_update_cons<RSV, MD, 1><<<L.grid_upd, HG_BLK, 0, s>>>(G, dtfac, ph);                 \
   k_update_c2p<RSV, MD><<<L.grid_upd, HG_BLK, 0, s>>>(G, sub, pf)
   if (G.mdim == 0) {
     if (G.rescale) { HG_UPD(true, 0); }
