@@ -88,7 +88,7 @@ WORKLOADS = {
                         label="torus192's initial state on the time-dependent metric path (metric_dim 3): the "
                               "Minkowski-spherical test spacetime, geometry of three time levels and the "
                               "finite-difference connection evaluated on the device every step, FP64"),
-    "pnbbh300": dict(kind="pnbbh", n=(300, 160, 400), ref_cfg="pnbbh_dynmink", ref_note=PN_REF_NOTE,
+    "pnbbh300": dict(kind="pnbbh", n=(300, 160, 400), ref_cfg="pnbbh_dynmink", ref_note=PN_REF_NOTE, ref_nblocks=64,
                      label="circumbinary disk of an equal-mass black-hole binary (the post-Newtonian binary disk "
                            "setup: separation 20M, r 0.75a-13a, beta 10 loop, H/R 0.1 cooling, 1% seeded noise) in "
                            "the first post-Newtonian binary metric evaluated on the device every substep "
@@ -647,7 +647,13 @@ def reference_arm(wl, ncores, warmup, steps, full_grid=False):
         return None, how
     n = wl["n"]
     procs = max(1, min(ncores, 64))
-    if min(n) > 1:
+    if min(n) > 1 and wl.get("ref_nblocks"):
+        # a bounded sample: the grid split into ref_nblocks equal blocks (the
+        # reference's dynamic path holds ~6 KB per zone, too much for one
+        # block per core of the whole grid in host memory), procs of them
+        counts, block = decompose(n, wl["ref_nblocks"])
+        layout = "%d of the %dx%dx%d blocks of %s" % ((procs,) + counts + ("x".join(map(str, block)),))
+    elif min(n) > 1:
         counts, block = decompose(n, procs)
         procs = counts[0] * counts[1] * counts[2]
         layout = "%dx%dx%d blocks of %s" % (counts + ("x".join(map(str, block)),))

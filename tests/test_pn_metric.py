@@ -217,3 +217,22 @@ def test_dynamic_grids_step_in_a_batch_as_alone():
         assert np.array_equal(e.download(), a.download())
         a.close()
         e.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["static", "dynamic", "dynamic_mixed"])
+def test_grid_bytes_accounts_for_the_allocation(kind):
+    """hg_grid_bytes (what the server admits grids by) against the device
+    memory an Engine actually takes, cudaMalloc's rounding aside."""
+    from coolharm3d_b200 import torus
+    if kind == "static":
+        d = torus.torus_desc((48, 40, 32))
+    else:
+        d = pnbbh.pnbbh_desc((48, 40, 32), precision=hg.PREC_MIXED if kind == "dynamic_mixed" else hg.PREC_FP64)
+    want = hg.grid_bytes(d)
+    free0, _ = hg.mem_info(0)
+    e = hg.Engine(d)
+    free1, _ = hg.mem_info(0)
+    took = free0 - free1
+    e.close()
+    assert abs(took - want) <= 0.05 * want + (64 << 20), (kind, took, want)
