@@ -338,6 +338,7 @@ def run_ours(args, wl, rank, world, device):
     e.step(args.warmup)
     # timed region: K steps on the device, state resident, each step one
     # CUDA-graph launch (no per-kernel events)
+    fails0 = e.fail_counts().astype(np.int64)
     clk = ClockSampler(device)
     clk.start()
     barrier()
@@ -347,6 +348,10 @@ def run_ours(args, wl, rank, world, device):
     barrier()
     clocks = clk.stop()
     ms = e.last_step_ms()
+    # failure counters (nfailtot) of the timed steps, per step: how many
+    # zones the inversion's fallback tree and the entropy fix took
+    dfail = e.fail_counts().astype(np.int64) - fails0
+    nfail_per_step = {nm: float(dfail[i]) / args.steps for i, nm in enumerate(hg.NFAIL_NAMES) if dfail[i]}
     # kernel classes: the same K steps again with an event before every kernel
     e.profile(True)
     e.step(args.steps)
@@ -424,6 +429,7 @@ def run_ours(args, wl, rank, world, device):
                   "d2h_bytes_per_step": float(state_bytes) / args.steps + 16 + 120}
     total_launches = sum(v[1] for v in kt.values()) + 2 * args.steps  # k_begin launches are in "misc"
     out["gpu_launches"] = int(sum(v[1] for v in kt.values()))
+    out["nfail_per_step"] = nfail_per_step
     if clocks:
         out["clocks"] = clocks
     if rank == 0 and args.mixed_steps > 0 and args.precision == "fp64":

@@ -31,6 +31,7 @@ void launch_face_flux(const GridDev &G, const LaunchCfg &L, cudaStream_t s, int 
 void launch_fixup_bounds(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_bounds_only(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 cudaError_t prepare_kernels();
+int fallback_blocks_per_sm(bool rs);
 void launch_geom_levels(const GridDev &G, const LaunchCfg &L, cudaStream_t s);
 void launch_conn_broadcast(const GridDev &G, const LaunchCfg &L, cudaStream_t s, const double *rows);
 void launch_totals(const GridDev &G, const LaunchCfg &L, cudaStream_t s, double *part, double *out);
@@ -47,6 +48,7 @@ void launch_step(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s, h
 void launch_geom_levels(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s);
 void launch_face_flux(const hg::GridDev &G, const hg::LaunchCfg &L, cudaStream_t s, int d);
 cudaError_t prepare_kernels();
+int fallback_blocks_per_sm(bool rs);
 }  // namespace hg_fma
 
 // One step's launch sequence of the grid's precision form.  The plain FP64
@@ -295,6 +297,11 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     h->L.grid_bnd = grid_for(faces - G.capacity, 16);
     h->L.strip_nf = 2;  // 2-face strips in all three directions (with these
     h->L.strip_x1 = 1;  // block counts, the torus's fastest)
+    {
+      const int fb = fma_kernels(G) ? hg_fma::fallback_blocks_per_sm(G.rescale != 0)
+                                    : hg::fallback_blocks_per_sm(G.rescale != 0);
+      h->L.grid_fb = (long)sms * fb > HG_BLK_CAP ? HG_BLK_CAP : sms * fb;
+    }
     ALLOC(G.blk, sizeof(double) * HG_BLK_CAP);
     if (cudaMallocHost((void **)&h->h_stage, (size_t)HG_XCH * HG_XCH_BYTES) != cudaSuccess) {
       cudaGetLastError();

@@ -125,6 +125,9 @@ static __device__ __noinline__ int utoprim_1d(const double *U, const Geom &g, do
 }
 
 // Utoprim_1d_ee (utoprim_1d_ee.c:156-847): W Newton with an inner rho Newton.
+// The two Newton loops are inlined into utoprim_1d_ee, so EEState lives in
+// registers instead of the stack for the whole nested iteration (the
+// fallback kernel's time is the longest of these chains).
 struct EEState {
   double Bsq, QdotBsq, Qtsq, Qdotn, D, Sc, rho_gm1, two_Bsq;
   double W_for_gnr2, rho_for_gnr2, W_for_gnr2_old, rho_for_gnr2_old, drho_dW;
@@ -132,7 +135,7 @@ struct EEState {
   double t2, t4, t7, t24, t300, t400, s100, s200;
 };
 
-static __device__ __noinline__ int ee_gnr2(EEState &s, double *x)  // gnr2 + func_rho (utoprim_1d_ee.c:640-847)
+static __device__ __forceinline__ int ee_gnr2(EEState &s, double *x)  // gnr2 + func_rho (utoprim_1d_ee.c:640-847)
 {
   double f = 1., df = 1., errx = 1.;
   int n_iter = 0, i_extra = 0, doing_extra = 0;
@@ -163,7 +166,7 @@ static __device__ __noinline__ int ee_gnr2(EEState &s, double *x)  // gnr2 + fun
   return 1;
 }
 
-static __device__ __noinline__ int ee_gnr(EEState &s, double *x)  // general_newton_raphson + func_W
+static __device__ __forceinline__ int ee_gnr(EEState &s, double *x)  // general_newton_raphson + func_W
 {
   double f = 1., df = 1., errx = 1.;
   int n_iter = 0, i_extra = 0, doing_extra = 0;

@@ -161,6 +161,7 @@ struct LaunchCfg {
   int grid_flux32;  // FP32 flux kernel of the mixed form (more resident blocks)
   int strip_nf;     // faces per thread of the strip flux kernels (1..3)
   int strip_x1;     // x1 faces in strips too (else one face per thread)
+  int grid_fb;      // k_fallback: every block the device holds at once (set by hg_init)
 };
 #define HG_BLK_CAP 65536  // largest grid of any kernel (the per-block M_tot partials are sized for it)
 

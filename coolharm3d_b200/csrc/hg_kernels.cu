@@ -1436,6 +1436,19 @@ static cudaError_t strip_attrs_rm()
   return e;
 }
 
+// Blocks of k_fallback one SM holds at once.  Each queued zone is one long
+// serial chain (nested Newton iterations), so the kernel is launched with
+// every block the device holds: up to that many threads, each zone runs in a
+// thread of its own instead of queueing behind another zone's chain.
+int fallback_blocks_per_sm(bool rs)
+{
+  int n = 0;
+  const cudaError_t e = rs ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fallback<true>, HG_BLK, 0)
+                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fallback<false>, HG_BLK, 0);
+  if (e != cudaSuccess) cudaGetLastError();
+  return (e == cudaSuccess && n > 0) ? n : 2;
+}
+
 // Kernel attributes that must be set before a launch (the strip kernels'
 // shared memory above the default limit), once per device, outside any
 // stream capture: called by hg_init.
@@ -1552,8 +1565,8 @@ static void launch_substep(const GridDev &G, const LaunchCfg &L, cudaStream_t s,
     if (G.rescale) k_ee_faces<true><<<L.grid_fix * 6, HG_BLK, 0, s>>>(G, ph, sub);
     else k_ee_faces<false><<<L.grid_fix * 6, HG_BLK, 0, s>>>(G, ph, sub);
   }
-  if (G.rescale) k_fallback<true><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
-  else k_fallback<false><<<L.grid_fix, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  if (G.rescale) k_fallback<true><<<L.grid_fb, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
+  else k_fallback<false><<<L.grid_fb, HG_BLK, 0, s>>>(G, sub, dtfac, ph, pf);
   mark(R, KC_BOUNDS, s);
   k_bounds<<<L.grid_bnd, HG_BLK, 0, s>>>(G, pf, 0, sub + 1);
   mark(R, KC_FIXUP, s);
