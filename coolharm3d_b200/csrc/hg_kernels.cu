@@ -53,15 +53,21 @@ namespace HG_KNS {
 using namespace hg;
 
 // register caps (minimum resident blocks of 128 threads per SM), measured on
-// the 192x192x128 torus: the flux and conserved-update kernels at 3 blocks
-// (168 registers, no spills; at 4 blocks, 128 registers, the flux kernels
-// spilled ~3e6 local-load sectors per launch: 6.36 against 6.70 ms per step),
-// the inversion at 4 (118 registers; 3 blocks spilled and measured slower)
+// the 192x192x128 torus: the flux kernels at 3 blocks (168 registers, no
+// spills; at 4 blocks, 128 registers, they spilled ~3e6 local-load sectors
+// per launch: 6.36 against 6.70 ms per step); the corrector's conserved
+// update at 3 blocks (168 registers; 4 blocks spill 264 bytes), the
+// predictor's at 4 (128 registers without spills); the inversion at 5 (96
+// registers, 112 bytes of spill stores) -- those two: 6.31 -> 6.24 ms per
+// step, the mixed form 4.25 -> 4.16
 #ifndef HG_CONS_MINB
 #define HG_CONS_MINB 3
 #endif
+#ifndef HG_CONS0_MINB
+#define HG_CONS0_MINB 4
+#endif
 #ifndef HG_C2P_MINB
-#define HG_C2P_MINB 4
+#define HG_C2P_MINB 5
 #endif
 #ifndef HG_FLUX_MINB
 #define HG_FLUX_MINB 3
@@ -553,7 +559,7 @@ __device__ __forceinline__ void update_zone(const GridDev &G, int i, int j, int 
 // takes it as a template parameter: each substep's kernel holds only its own
 // source path (fewer registers, no spill at the 3-block cap).
 template <bool RS, int MDIM, int SUB>
-__global__ void __launch_bounds__(HG_BLK, HG_CONS_MINB) k_update_cons(const __grid_constant__ GridDev G,
+__global__ void __launch_bounds__(HG_BLK, SUB == 0 ? HG_CONS0_MINB : HG_CONS_MINB) k_update_cons(const __grid_constant__ GridDev G,
                                                                     double dtfac, const double *__restrict__ p_h)
 {
   constexpr int sub = SUB;
