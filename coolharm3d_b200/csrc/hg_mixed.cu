@@ -22,7 +22,11 @@
 namespace hg {
 
 #ifndef HG_FLUX32_MINB
-#define HG_FLUX32_MINB 6  // blocks of 128 per SM for the FP32 flux kernels (80 registers)
+// blocks of 128 per SM for the FP32 flux kernels: 7 (72 registers, a few
+// dozen bytes of spills in the strip kernels) took the mixed torus step
+// from 4.18 to 4.15 ms against 6 (80 registers); 8 (64 registers) changed
+// results in the shock tube, where U3 and B3 must stay exactly zero
+#define HG_FLUX32_MINB 7
 #endif
 
 // The face's geometry in float: the entries get_state and vchar_fast read
