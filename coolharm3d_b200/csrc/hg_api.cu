@@ -297,10 +297,11 @@ extern "C" int hg_init(const hg_grid_desc *desc, hg_handle **out)
     h->L.grid_bnd = grid_for(faces - G.capacity, 16);
     h->L.strip_nf = 2;  // 2-face strips in all three directions (with these
     h->L.strip_x1 = 1;  // block counts, the torus's fastest)
-    {
+    {  // the fallback tree: every block the device holds at once, no more
+       // than the grid's zones need (small grids in a batch launch few)
       const int fb = fma_kernels(G) ? hg_fma::fallback_blocks_per_sm(G.rescale != 0)
                                     : hg::fallback_blocks_per_sm(G.rescale != 0);
-      h->L.grid_fb = (long)sms * fb > HG_BLK_CAP ? HG_BLK_CAP : sms * fb;
+      h->L.grid_fb = grid_for(G.capacity, fb);
     }
     ALLOC(G.blk, sizeof(double) * HG_BLK_CAP);
     if (cudaMallocHost((void **)&h->h_stage, (size_t)HG_XCH * HG_XCH_BYTES) != cudaSuccess) {

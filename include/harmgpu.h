@@ -252,9 +252,11 @@ int hg_get_totals(hg_handle *h, double U_tot[8], double F_tot[48], double *divb_
  * fastest per kernel class: it saves the resident state, runs `steps` steps
  * per candidate (per class: 8 block counts, and 3 strip lengths for the
  * flux), puts the state back, and returns the chosen configuration with the
- * device time per step before and after.  The results of a step do not
- * depend on the configuration (M_tot's per-block partial sums aside).  No
- * reference counterpart. */
+ * device time per step before and after.  grid_fixup sets the entropy
+ * faces' and the fixups' launches; the fallback tree's own launch is not
+ * configurable (every block the device holds at once, up to the grid's
+ * zones).  The results of a step do not depend on the configuration
+ * (M_tot's per-block partial sums aside).  No reference counterpart. */
 typedef struct hg_launch_config {
   int32_t grid_flux, grid_flux32, grid_emf, grid_update, grid_fixup, grid_bounds;
   int32_t strip_faces;          /* faces per thread of the strip flux kernels, 1..3 */
