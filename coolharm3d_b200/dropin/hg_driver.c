@@ -1,7 +1,7 @@
 /* hg_driver.c -- the HARM3D driver's side of libharmgpu: compiled into the
  * reference's own build (next to main.c and step_ch.c, with its decs.h) when
- * USE_GPU_STEP is 1.  Five hooks connect it (INTEGRATION.md shows the
- * patch, tests/test_dropin.py applies it and compares the result):
+ * USE_GPU_STEP is 1.  Five hooks connect it (tests/test_dropin.py applies
+ * them to the reference's sources and compares the result):
  *
  *   main.c, after global_init():     hg_gpu_init();        the grid goes to the GPU
  *   step_ch.c, top of step_ch():     if (hg_gpu_step()) return;
